@@ -1,0 +1,232 @@
+/*
+ * fcc.h — C ABI of the B200-native Fourier contour cell time step.
+ *
+ * This is the drop-in boundary for the hot path of FourierContourCells.jl: the
+ * Julia API `Simulation`, `step!`, `run!`, `compute_gradients!`, `shape_index`
+ * (src/FourierContourCells.jl:55-76) becomes a handle plus plain-pointer calls
+ * that a Julia `ccall` shim (or Python ctypes) binds.  No C++ or torch types
+ * cross this boundary.
+ *
+ * Conventions that follow the reference so that its callers need no changes:
+ *   - body, type and parent ids are 1-based, as in `Bodies` (src/bodies.jl:62-86);
+ *   - per-body matrices are column-major with one column per body, e.g. `coef`
+ *     is ncoef x N with column i = [a0; a2..aM; b2..bM] of body i
+ *     (src/basis.jl:10-14, src/bodies.jl:56), contour arrays are ntheta x N;
+ *   - every floating-point value crosses the ABI as double and is converted to
+ *     the simulation precision on the way in, as `convert_precision` and
+ *     `_convert_eltype` do (src/energies/interface.jl:220-257,
+ *     src/simulation.jl:312);
+ *   - errors are status codes; FCC_ERR_ARGUMENT and FCC_ERR_DIMENSION are
+ *     raised exactly where the reference throws ArgumentError and
+ *     DimensionMismatch, and fcc_last_error() returns the message.
+ *
+ * Ownership: the library copies host arrays in and owns every device buffer;
+ * getters copy out into caller buffers.  Each handle owns one CUDA stream.
+ * Handles are independent: concurrent handles on separate host threads give
+ * the same results as sequential runs (test/test_cuda.jl:187-196).
+ */
+#ifndef FCC_H
+#define FCC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FCC_MAX_TYPES 8   /* body types per simulation (BodyType table) */
+#define FCC_MAX_TERMS 16  /* energy terms per simulation */
+#define FCC_MAX_MODES 9   /* shape modes n = 2..10, i.e. maxmode <= 10 */
+
+typedef int32_t fcc_status;
+enum {
+    FCC_OK = 0,
+    FCC_ERR_ARGUMENT = 1,    /* reference: ArgumentError */
+    FCC_ERR_DIMENSION = 2,   /* reference: DimensionMismatch */
+    FCC_ERR_CUDA = 3,        /* CUDA runtime error (message has the CUDA text) */
+    FCC_ERR_UNSUPPORTED = 4, /* valid model outside this build's kernels */
+    FCC_ERR_DEVICE = 5,      /* device-side error status (e.g. non-finite state) */
+    FCC_ERR_NOMEM = 6        /* device allocation failed */
+};
+
+/* Energy term kinds (src/energies/body_terms.jl, contact.jl, bonds.jl). */
+enum {
+    FCC_TENSION = 1,               /* Tension(eta):           a = eta            */
+    FCC_PERIMETER_ELASTICITY = 2,  /* PerimeterElasticity(l, p0): a = l, b = p0 */
+    FCC_OVERLAP = 3,               /* Overlap(J; related):    J, Jrel tables     */
+    FCC_LINEAR_REPULSION = 4,      /* LinearRepulsion(k):     a = k              */
+    FCC_HARMONIC_BOND = 5          /* HarmonicBond(k; r0):    a = k, b = r0      */
+};
+
+/* One energy term.  `ntypes_on > 0` wraps the term in OnTypes(term, types_on...)
+ * (src/energies/interface.jl:278-298).  Overlap couplings are nJ x nJ tables,
+ * column-major, indexed (type_i, type_j) like the reference's SMatrix
+ * (src/energies/contact.jl:12-28); a scalar coupling is nJ = 1. */
+typedef struct {
+    int32_t kind;
+    int32_t ntypes_on;
+    int32_t types_on[FCC_MAX_TYPES];
+    double a, b;
+    int32_t nJ;
+    double J[FCC_MAX_TYPES * FCC_MAX_TYPES];
+    double Jrel[FCC_MAX_TYPES * FCC_MAX_TYPES];
+} fcc_term;
+
+/* BodyType(; v0, Dr, Dt, mu_r, mu_theta, mu_ab, drag) (src/bodies.jl:30-45);
+ * parent_drag = 1 is drag = :parent. */
+typedef struct {
+    double v0, Dr, Dt, mu_r, mu_theta, mu_ab;
+    int32_t parent_drag;
+} fcc_body_type;
+
+/* Keyword arguments of Simulation(bodies, box; ...) (src/simulation.jl:66-68). */
+typedef struct {
+    double Lx, Ly;            /* PeriodicBox(Lx, Ly) */
+    double dt;                /* time step (default 0.005) */
+    int32_t ntheta;           /* contour nodes nθ (default 40) */
+    int32_t precision;        /* 64: Float64; 32: Float32 bulk, FP64 a0/projection/observables */
+    uint64_t seed;            /* Philox key (src/random.jl:103) */
+    double skin;              /* Verlet skin (default 0.3) */
+    int32_t ntypes;
+    const fcc_body_type* types;
+    int32_t nterms;
+    const fcc_term* terms;
+    int64_t nbonds;           /* bonds = [(i, j), ...]; 2*nbonds 1-based ids */
+    const int32_t* bonds;
+    int32_t nl_capacity;      /* initial neighbour-list capacity (0: 32, as NeighborList) */
+} fcc_params;
+
+/* Host body state, the fields of Bodies (src/bodies.jl:62-72). */
+typedef struct {
+    int64_t n;
+    int32_t ncoef;            /* 2K + 1, K = maxmode - 1 */
+    double* x;
+    double* y;
+    double* theta;
+    int32_t* imgx;
+    int32_t* imgy;
+    double* coef;             /* ncoef x n, column-major */
+    double* R0;
+    int32_t* type;            /* 1-based */
+    int32_t* parent;          /* 1-based */
+} fcc_bodies_host;
+
+/* Gradient buffers of Gradients (src/gradients.jl:15-38).  Any pointer may be
+ * NULL to skip that field. */
+typedef struct {
+    double* GR;      /* ntheta x n, dE/dR */
+    double* GD;      /* ntheta x n, dE/dR' */
+    double* GDD;     /* ntheta x n, dE/dR'' */
+    double* P;       /* ntheta x n, contact energy density */
+    double* gx;      /* n */
+    double* gy;      /* n */
+    double* gtheta;  /* n */
+    double* glab;    /* ncoef x n, dE/dlab / R0 */
+    double* gcoef;   /* ncoef x n, body-frame gradient, row 1 = raw dE/da0 */
+    double* Ebody;   /* n */
+} fcc_gradients_host;
+
+/* Derived geometry of Geometry (src/geometry.jl:13-32); NULL skips a field. */
+typedef struct {
+    double* lab;     /* ncoef x n */
+    double* labR0;   /* ncoef x n */
+    double* R;       /* ntheta x n */
+    double* dR;      /* ntheta x n */
+    double* ddR;     /* ntheta x n */
+    double* rmax;    /* n */
+} fcc_geometry_host;
+
+/* Cell list and neighbour list (src/neighbors.jl:16-33, 110-127), 1-based as
+ * in the reference.  Arrays are sized by the caller from fcc_neighbor_dims. */
+typedef struct {
+    int32_t* cellid;  /* n, cx + ncx*cy + 1 */
+    int32_t* perm;    /* n, bodies sorted stably by cellid */
+    int32_t* start;   /* ncx*ncy, empty cells: start = 1, stop = 0 */
+    int32_t* stop;    /* ncx*ncy */
+    int32_t* idx;     /* cap x n, neighbours of body i in column i */
+    int32_t* count;   /* n */
+} fcc_neighbors_host;
+
+typedef struct fcc_sim fcc_sim;
+
+/* Callback of fcc_run, called every `every` steps (src/simulation.jl:220-235). */
+typedef void (*fcc_callback)(fcc_sim* sim, void* user);
+
+/* Simulation(bodies, box; ...): src/simulation.jl:66-105.  Copies `bodies`
+ * to the device, enforces the shape constraints and builds the geometry. */
+fcc_status fcc_create(const fcc_params* params, const fcc_bodies_host* bodies, fcc_sim** out);
+fcc_status fcc_destroy(fcc_sim* sim);
+
+/* step!(sim, n): src/simulation.jl:165-173 (eager launches, one host sync at the end). */
+fcc_status fcc_step(fcc_sim* sim, int64_t n);
+
+/* run!(sim, n; every, callback, graph): src/simulation.jl:220-235 and the CUDA
+ * graph driver ext/FourierContourCellsCUDAExt.jl:144-180.  Results equal fcc_step. */
+fcc_status fcc_run(fcc_sim* sim, int64_t n, int64_t every, fcc_callback cb, void* user, int32_t graph);
+
+/* update_neighbors!(sim; force): src/simulation.jl:132-142. */
+fcc_status fcc_update_neighbors(fcc_sim* sim, int32_t force);
+
+/* compute_gradients!(sim): src/simulation.jl:150-158 (frame = true). */
+fcc_status fcc_compute_gradients(fcc_sim* sim);
+
+/* The fields of sim.bodies plus the device clock (Philox draw index), sim.t and sim.step. */
+fcc_status fcc_get_state(fcc_sim* sim, fcc_bodies_host* out, int64_t* clock, double* t, int64_t* step);
+
+/* Overwrite the body state (x, y, theta, imgx, imgy, coef; R0, type and parent
+ * must match the created ones) and the clock; then enforce_shape!,
+ * update_geometry! and an invalidated neighbour list, like the tests' refresh!
+ * (test/runtests.jl:9-15). `clock < 0` keeps the clock. */
+fcc_status fcc_set_state(fcc_sim* sim, const fcc_bodies_host* in, int64_t clock);
+
+/* sim.dt = dt (test/test_cuda.jl:156-162). */
+fcc_status fcc_set_dt(fcc_sim* sim, double dt);
+
+fcc_status fcc_get_gradients(fcc_sim* sim, const fcc_gradients_host* out);
+fcc_status fcc_get_geometry(fcc_sim* sim, const fcc_geometry_host* out);
+
+/* Sizes for fcc_get_neighbors: grid cells, capacity, and sim.neighbors.builds. */
+fcc_status fcc_neighbor_dims(fcc_sim* sim, int32_t* ncx, int32_t* ncy, int32_t* cap, int64_t* builds, int32_t* valid);
+fcc_status fcc_get_neighbors(fcc_sim* sim, const fcc_neighbors_host* out);
+
+/* perimeters / areas / shape_index (src/observables.jl:7-18), FP64 node sums
+ * on the device.  type = 0: all bodies; else bodies of that type, in body
+ * order; *count receives the number of values written. */
+fcc_status fcc_perimeters(fcc_sim* sim, int32_t type, double* out, int64_t* count);
+fcc_status fcc_areas(fcc_sim* sim, int32_t type, double* out, int64_t* count);
+fcc_status fcc_shape_index(fcc_sim* sim, int32_t type, double* out, int64_t* count);
+
+/* body_energy(sim): src/observables.jl:47 (sum of Ebody of the last gradient evaluation). */
+fcc_status fcc_body_energy(fcc_sim* sim, double* out);
+
+/* philox_noise!(xi, key, n): src/random.jl:113-130.  Fills out (3 x nbodies,
+ * column-major) with the first three standard normals of philox_normals for
+ * bodies 1..nbodies and draw index `draw`, in precision 32 or 64. */
+fcc_status fcc_philox_noise(uint64_t seed, uint64_t draw, int64_t nbodies, int32_t precision, double* out);
+
+/* Standalone neighbour build on caller arrays (no simulation handle):
+ * update_celllist! + the neighbour kernel (src/neighbors.jl:81-92, 148-174) on
+ * x, y, rmax (length n, precision 32 or 64).  `range` is the contact range
+ * plus skin.  Outputs are 1-based; count[i] may exceed cap (overflow, as the
+ * reference's kernel counts without storing).  Grid sizes follow
+ * CellList(box, cutoff, n).  Device scratch is allocated per call. */
+fcc_status fcc_build_neighbors(int32_t precision, int64_t n, const double* x, const double* y,
+                               const double* rmax, double Lx, double Ly, double cutoff, double range,
+                               int32_t cap, int32_t* cellid, int32_t* perm, int32_t* start,
+                               int32_t* stop, int32_t* idx, int32_t* count);
+
+/* Device timing of the last fcc_step/fcc_run call (CUDA events on the handle's
+ * stream): elapsed milliseconds, launches of this library's kernels, and
+ * steps executed. */
+fcc_status fcc_last_timing(fcc_sim* sim, double* ms, int64_t* launches, int64_t* steps);
+
+/* Message of the last error on this thread. */
+const char* fcc_last_error(void);
+
+/* Library build tag (architecture and kernel variants). */
+const char* fcc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FCC_H */
