@@ -1,0 +1,329 @@
+"""Benchmark of the B200 time step: body-steps/s of the N = 16384 FP32 monolayer.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Workload (the metric's configuration): hexagonal_monolayer(128, 128;
+packing = 0.95), R0 ~ Normal(1, 0.1) clipped to [0.8, 1.2], modes 2..10,
+nθ = 40, Tension(0.01) + Overlap(1.0) + PerimeterElasticity(0.1, 3.7),
+v0 = 0.06, Dr = 0.01, μab = 0.1, dt = 0.005, FP32 (FP64 a0 / projection),
+synthetic seeded state (no dataset exists for this model).
+
+A "step" is one time step of the whole monolayer.  `value` is device-timed
+(CUDA events on the library's stream around the persistent multi-step
+launches), `e2e` the same metric through the C ABI with host buffers
+(set_state from host arrays, run, get_state to host arrays) under a wall
+clock.  Under torchrun every rank runs an independent replica (different
+seed): the path does not shard, so there is no collective in the data path;
+the job time is the max over ranks.
+
+`--impl reference` times the reference's CPU path on the host cores: the
+C++ restatement of it (the oracle), since the Julia reference cannot run in
+this image.
+"""
+
+import argparse
+import importlib.util
+import json
+import math
+import os
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+N_SIDE = 128
+WORKLOAD = "hexagonal_monolayer(128,128) N=16384 FP32, Tension(0.01)+Overlap(1.0)+PerimeterElasticity(0.1,3.7)"
+METRIC = "body-steps/s at N=16384 FP32"
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "step_kernel_n16384.json")
+
+
+def load_package():
+    name = "fcc_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    pkg = os.path.join(ROOT, "fouriercontourcells.jl_b200")
+    spec = importlib.util.spec_from_file_location(name, os.path.join(pkg, "__init__.py"), submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_oracle():
+    """The CPU oracle (bench's CPU-baseline leg only)."""
+    name = "fcc_oracle"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "oracle", "oracle.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload(fcc, seed=1234):
+    bodies, box = fcc.polydisperse_monolayer(N_SIDE, N_SIDE, packing=0.95, maxmode=10, seed=seed)
+    kw = dict(types=(fcc.BodyType(v0=0.06, Dr=0.01, μab=0.1),),
+              energies=(fcc.Tension(0.01), fcc.Overlap(1.0), fcc.PerimeterElasticity(0.1, 3.7)), dt=0.005, seed=seed)
+    return bodies, box, kw
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """SM clocks and throttle reasons of one GPU during the timed region."""
+
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap",
+               0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, index):
+        self.index, self.samples, self.reasons, self.max_mhz = index, [], set(), None
+        self._stop = threading.Event()
+        self._t = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nvml = None
+
+    def _loop(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nvml.nvmlDeviceGetClockInfo(self.h, self.nvml.NVML_CLOCK_SM))
+                r = self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.reasons.update(n for b, n in self.REASONS.items() if r & b)
+            except Exception:
+                pass
+            self._stop.wait(0.05)
+
+    def __enter__(self):
+        if self.nvml:
+            self._t = threading.Thread(target=self._loop, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+
+    def summary(self):
+        med = float(np.median(self.samples)) if self.samples else None
+        return {"sm_mhz": med, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------ algorithmic work
+def algorithmic_per_body_step(tests_per_body, hits_per_body, nθ=40, ncoef=19, K=9):
+    """FP32 flops and compulsory HBM bytes of one body-step (the definitions
+    behind the roofline; counts of node-neighbour tests and hits come from the
+    oracle on the same state)."""
+    flops = (2 * 2 * nθ * ncoef      # synthesis of R, R' (the reference's S*labR0 rows needed)
+             + 2 * 2 * nθ * ncoef    # pullback glab = C'GR + D'GD
+             + 12 * nθ               # body terms (q, Q, W R/q, W R'/q)
+             + 10 * tests_per_body   # minimum image + distance test per node-neighbour pair
+             + (8 * K + 8) * hits_per_body  # R_j(psi) recurrence and depth per hit
+             + 12 * nθ               # contact gradient, force and torque per node
+             + 30 * K + 60)          # body frame, update, constraints, lab frame
+    # own record read + next record write (96 B each), coefficients r/w, neighbour
+    # list (count + ~6 ids), R0, forces/energy written
+    bytes_ = 96 + 96 + 2 * 76 + 4 * (1 + 6) + 4 + 16
+    return flops, bytes_
+
+
+def flush_l2():
+    import torch
+    buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+    buf.fill_(1.0)
+    torch.cuda.synchronize()
+    del buf
+
+
+# ------------------------------------------------------------------ arms
+def cpu_baseline(fcc, oracle, budget_s=15.0, max_steps=200):
+    """The oracle (FP64, OpenMP on all host cores) on the same workload,
+    for a bounded number of steps (about `budget_s` seconds)."""
+    threads = oracle.set_threads(0)
+    bodies, box, kw = workload(fcc)
+    sim = oracle.OracleSimulation(bodies, box, T=np.float64, **kw)
+    sim.step(1)  # first step builds the neighbour list
+    t0 = time.perf_counter()
+    sim.step(1)
+    one = time.perf_counter() - t0
+    steps = int(max(2, min(max_steps, budget_s / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    sim.step(steps)
+    dt = time.perf_counter() - t0
+    v = bodies.n * steps / dt
+    return {"value": v, "unit": "body-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{steps} FP64 steps of the N={bodies.n} workload on {threads} threads (C++ restatement of the reference CPU path)"}, sim
+
+
+def reference_arm(args):
+    """--impl reference: rank 0 times the reference CPU path (its C++
+    restatement) on the bench workload."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    fcc = load_package()
+    oracle = load_oracle()
+    budget = float(os.environ.get("FCC_REF_BUDGET_S", "60"))
+    per = max(1.0, budget / max(1, args.warmup + args.steps))
+    threads = oracle.set_threads(0)
+    bodies, box, kw = workload(fcc)
+    sim = oracle.OracleSimulation(bodies, box, T=np.float64, **kw)
+    sim.step(1)
+    t0 = time.perf_counter()
+    sim.step(1)
+    one = time.perf_counter() - t0
+    # every bench step is a bounded sample: as many time steps of the full
+    # monolayer as fit into the per-step budget (at least one)
+    k = max(1, int(per / max(one, 1e-6)))
+    for _ in range(args.warmup):
+        sim.step(1)
+    nsteps = min(args.steps, max(1, int(budget / max(one * k, 1e-6))))
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        sim.step(k)
+    dt = time.perf_counter() - t0
+    value = bodies.n * k * nsteps / dt
+    line = {"metric": METRIC, "value": value, "unit": "body-steps/s", "n_gpus": args.gpus, "steps": nsteps,
+            "warmup": args.warmup, "ms_per_step": dt / (k * nsteps) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD.replace("FP32", "FP64 (reference CPU path)"), "n": bodies.n, "nθ": 40},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "body-steps/s", "cores": threads, "kind": "port",
+                             "sample": f"{nsteps} samples of {k} FP64 time steps of the N={bodies.n} workload "
+                                       f"(C++ restatement of the reference CPU path; Julia is not in the image)"},
+            "e2e": {"value": value, "unit": "body-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def gpu_arm(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    fcc = load_package()
+    bodies, box, kw = workload(fcc, seed=1234 + rank)
+    sim = fcc.Simulation(bodies, box, T=np.float32, **kw)
+    N = bodies.n
+
+    # warm-up (also builds the neighbour list and settles the rebuild cadence)
+    sim.run(max(3, args.warmup))
+    flush_l2()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        sim.run(args.steps)
+        torch.cuda.synchronize()
+    ms, launches, steps = sim.last_timing()
+    if dist:
+        dist.barrier()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * N * steps / (ms_max * 1e-3)
+
+    # end to end through the C ABI with host buffers (wall clock, max over ranks)
+    host = sim.bodies
+    h2d = sum(getattr(host, f).nbytes for f in ("x", "y", "θ", "imgx", "imgy", "coef"))
+    d2h = sum(getattr(host, f).nbytes for f in ("x", "y", "θ", "imgx", "imgy", "coef", "R0", "type", "parent"))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim.set_state(host)
+    sim.run(args.steps)
+    out = sim.bodies
+    e2e_s = time.perf_counter() - t0
+    assert np.isfinite(out.x).all()
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e = world * N * args.steps / float(te.item())
+
+    if rank == 0:
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        hbm_peak = peaks.get("hbm_gbs", 6650.0)
+        peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+        # work counters of the state the timed steps ran on (oracle, same state)
+        oracle = load_oracle()
+        osim = oracle.OracleSimulation(out, box, T=np.float64, **kw)
+        osim.refresh()
+        tests, hits, _ = osim.contact_counters()
+        flops_b, bytes_b = algorithmic_per_body_step(tests / N, hits / N)
+        launch_ms = ms / max(1, launches)
+        steps_per_launch = steps / max(1, launches)
+        bytes_launch = bytes_b * N * steps_per_launch
+        achieved_gbs = bytes_launch / (launch_ms * 1e-3) / 1e9
+        traffic = None
+        try:
+            prof = json.load(open(PROFILE_SUMMARY))
+            traffic = prof["dram_bytes_per_step"] * steps_per_launch
+        except Exception:
+            pass
+        cs = clk.summary()
+        sm_mhz = cs["sm_mhz"] or 1965.0
+        fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+        achieved_tf = flops_b * N * steps_per_launch / (launch_ms * 1e-3) / 1e12
+        cpu, _ = cpu_baseline(fcc, oracle)
+        line = {
+            "metric": METRIC, "value": value, "unit": "body-steps/s", "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": N, "nθ": 40, "modes": "2..10", "parallelism": f"replicas{world}",
+                       "steps_per_launch": steps_per_launch,
+                       "l2": "flushed before the timed region; state (3.5 MB) is L2-resident by design and each step "
+                             "reads the previous step's output"},
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved_gbs / hbm_peak, "traffic": traffic,
+                         "peak_source": f"{peak_src} hbm_gbs",
+                         "note": "compulsory bytes per body-step; the step is FP32-issue bound (roofline_fp32)"},
+            "roofline_fp32": {"bound": "fp32", "achieved": achieved_tf, "peak": fp32_peak, "unit": "TFLOP/s",
+                              "frac": achieved_tf / fp32_peak, "flops_per_body_step": flops_b,
+                              "peak_source": "nominal 148 SM x 128 FP32 lanes x 2 at the sampled SM clock"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": "body-steps/s", "h2d_bytes_per_step": h2d / args.steps,
+                    "d2h_bytes_per_step": d2h / args.steps,
+                    "api": "fcc_set_state(host) + fcc_run(K) + fcc_get_state(host), wall clock"},
+            "gpu_launches": launches * world,
+            "clocks": cs,
+            "builds": sim.builds,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

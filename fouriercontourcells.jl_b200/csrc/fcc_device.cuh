@@ -1,0 +1,321 @@
+// fcc_device.cuh — device data layout and helpers of the B200 time step.
+//
+// Layout in HBM (all bodies of all simulations of one engine, global body
+// index g; a single Simulation is an engine with one simulation):
+//
+//   rec[2][g][24]  geometry record, ping-pong by the parity of the
+//                  simulation's clock (current = clock & 1).  Neighbours
+//                  read it, so a step reads rec[cur] and writes rec[cur^1]:
+//                    [0] x  [1] y  [2] rmax  [3] w = parent_global<<3 | (type-1)
+//                    [4] R0*a0  [5..13] R0*alpha_n  [14..22] R0*beta_n  [23] theta
+//                  (lab-frame coefficients scaled by R0, src/geometry.jl:208-227;
+//                  modes n = 2..10 at fixed slots, unused modes stay zero).
+//                  96 B (FP32) per body = six 16-byte vector loads.
+//   coef[g][19]    body-frame coefficients [a0; a_2..a_10; b_2..b_10], owned
+//                  by body g and updated in place.
+//   imgx, imgy     periodic image counters (in place).
+//   nb_idx[g][cap], nb_count[g]   neighbour lists, body-major like the
+//                  reference's cap x N column-major matrix (neighbors.jl:110).
+//   cellid/slot/perm/cstart/cstop/ccount   counting-sort cell list.
+//
+// Kernels never read `rec` through the non-coherent (texture) path: the
+// persistent step kernel rewrites it between grid barriers.
+
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fcc {
+
+constexpr int KM = 9;        // shape modes n = 2..10
+constexpr int NCM = 2 * KM + 1;
+constexpr int RECW = 24;     // record width (values)
+constexpr int MT = 8;        // max body types
+constexpr int MTERM = 16;    // max terms
+constexpr double SHAPE_BOUND = 0.816496580927726;  // sqrt(2/3), src/dynamics.jl:26
+
+// record slots
+constexpr int R_X = 0, R_Y = 1, R_RMAX = 2, R_W = 3, R_A0 = 4, R_AL = 5, R_BE = 14, R_TH = 23;
+
+// per-simulation flags
+enum : int {
+    F_REBUILD = 1,     // skin exceeded: rebuild before the next force evaluation
+    F_FROZEN = 2,      // neighbour overflow: steps do nothing until the host regrows the list
+    F_VALID = 4,       // neighbour list built
+    F_NEED = 8,        // rebuild at the start of the next step
+    F_ACTIVE = 16,     // slot holds a simulation
+    F_NONFINITE = 32,  // a body state became non-finite
+    F_CONTACT = 64,    // simulation has contact terms (uses neighbour lists)
+};
+
+enum : int { BT_TENSION = 1, BT_PERIMETER = 2 };
+
+template <class T>
+struct SimDesc {
+    T Lx, Ly, invLx, invLy;
+    T dt, skin, nbrange, crange, dphi;  // nbrange = contact range + skin
+    T wx, wy;
+    int ncx, ncy, cell_off, ncells;
+    int body_off, n, nth, K;
+    uint32_t k0, k1;  // Philox key
+    int ntypes, rewrap, has_contact, has_parent_drag;
+    int nbt, nbd;
+    T v0[MT], Dr[MT], Dt[MT], mur[MT], muth[MT], muab[MT];
+    int parent_drag[MT];
+    int bt_kind[MTERM];
+    uint32_t bt_mask[MTERM];
+    T bt_a[MTERM], bt_b[MTERM];  // Tension: a = eta; PerimeterElasticity: a = lambda, b = p0*sqrt(pi)
+    T cA[2][MT][MT];             // summed Overlap couplings [related][ti][tj] (applied at d >= 0)
+    T cB[MT];                    // summed LinearRepulsion k of terms applying to ti (k*d at d > 0)
+    uint32_t bd_mask[MTERM];
+    T bd_k[MTERM], bd_r0[MTERM];
+};
+
+struct GridSync {
+    unsigned count;
+    unsigned gen;
+    int error;      // 1: a barrier wait ran out (the kernel returned early)
+    int any_need;   // some simulation rebuilds its neighbour list this step
+};
+
+template <class T>
+struct DevPtrs {
+    const SimDesc<T>* sims;
+    int nsims, Ntot, Ctot, nth, cap;
+    const int* sim_of;
+    T* rec0;
+    T* rec1;
+    T* coef;
+    int* imgx;
+    int* imgy;
+    const T* R0;
+    T* x0;
+    T* y0;
+    T* rmax0;
+    int* nb_idx;
+    int* nb_count;
+    int* cellid;
+    int* slot;
+    int* perm;
+    int* cstart;
+    int* cstop;
+    int* ccount;
+    const int* cell_sim;
+    int ccap;
+    const int* ch_idx;
+    const int* ch_count;
+    int bcap;
+    const int* bd_idx;
+    const int* bd_count;
+    int* flags;
+    long long* clock;
+    long long* builds;
+    int* maxcount;
+    GridSync* sync;
+    const T* cs;  // cos/sin of the node angles, 2*nth
+    // forces of the split (parent drag) step and of compute_gradients
+    T* gx;
+    T* gy;
+    T* gth;
+    T* glab;  // [g][19]
+    T* E;
+    // diagnostics of compute_gradients (ntheta per body) and the body-frame gradient
+    T* P;
+    T* GR;
+    T* GD;
+    T* GDD;
+    T* gcoef;  // [g][19]
+};
+
+// ------------------------------------------------------------ arithmetic
+// Exactly rounded single operations (no FMA contraction) for the integer
+// decisions that must agree bit for bit with the oracle: cell index,
+// neighbour test, skin test, wrap.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float t_rint(float a) { return rintf(a); }
+__device__ __forceinline__ double t_rint(double a) { return rint(a); }
+__device__ __forceinline__ float t_floor(float a) { return floorf(a); }
+__device__ __forceinline__ double t_floor(double a) { return floor(a); }
+__device__ __forceinline__ float t_sqrt(float a) { return sqrtf(a); }
+__device__ __forceinline__ double t_sqrt(double a) { return sqrt(a); }
+__device__ __forceinline__ float t_log(float a) { return logf(a); }
+__device__ __forceinline__ double t_log(double a) { return log(a); }
+__device__ __forceinline__ void t_sincos(float a, float* s, float* c) { sincosf(a, s, c); }
+__device__ __forceinline__ void t_sincos(double a, double* s, double* c) { sincos(a, s, c); }
+__device__ __forceinline__ float t_pi(float*) { return 3.14159265358979323846f; }
+__device__ __forceinline__ double t_pi(double*) { return 3.14159265358979323846; }
+
+// minimum_image, src/box.jl:14, exactly rounded as the reference evaluates it
+template <class T>
+__device__ __forceinline__ T minimum_image_exact(T d, T L) {
+    return sub_rn(d, mul_rn(L, t_rint(div_rn(d, L))));
+}
+// minimum image with a precomputed 1/L (force evaluation; differs from the
+// exact form only when d/L rounds across a half-integer, i.e. at distances
+// ~L/2 that the contact pre-check rejects)
+template <class T>
+__device__ __forceinline__ T minimum_image_fast(T d, T L, T invL) {
+    return d - L * t_rint(d * invL);
+}
+
+// wrap, src/box.jl:21-30
+template <class T>
+__device__ __forceinline__ T wrap_exact(T x, T L, int& shift) {
+    T s = t_floor(div_rn(x, L));
+    T xp = sub_rn(x, mul_rn(s, L));
+    if (xp >= L) {
+        xp = T(0);
+        s = add_rn(s, T(1));
+    }
+    shift = (int)s;
+    return xp;
+}
+
+// record field w <-> (parent, type)
+__device__ __forceinline__ float pack_w(int v, float*) { return __int_as_float(v); }
+__device__ __forceinline__ double pack_w(int v, double*) { return (double)v; }
+__device__ __forceinline__ int unpack_w(float w) { return __float_as_int(w); }
+__device__ __forceinline__ int unpack_w(double w) { return (int)w; }
+
+// ---------------------------------------------------------------- Philox
+// Philox4x32-10 (src/random.jl:15-36).
+__device__ __forceinline__ void philox(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t lo0 = 0xD2511F53u * c[0], hi0 = __umulhi(0xD2511F53u, c[0]);
+        uint32_t lo1 = 0xCD9E8D57u * c[2], hi1 = __umulhi(0xCD9E8D57u, c[2]);
+        uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0;
+        c[1] = lo1;
+        c[2] = n2;
+        c[3] = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+// src/random.jl:42-44
+__device__ __forceinline__ float uniform_open(float*, uint32_t a, uint32_t) {
+    return ((float)(a >> 9) + 0.5f) * 0x1p-23f;
+}
+__device__ __forceinline__ double uniform_open(double*, uint32_t a, uint32_t b) {
+    return ((double)(((((uint64_t)a) << 32) | b) >> 12) + 0.5) * 0x1p-52;
+}
+
+// Two standard normals of body i (1-based within its simulation) in draw n
+// from Philox block `block` (src/random.jl:47-51, 75-78).
+template <class T>
+__device__ __forceinline__ void philox_pair(uint32_t k0, uint32_t k1, uint32_t i, uint64_t n, uint32_t block, T& z1,
+                                            T& z2) {
+    uint32_t c[4] = {i, (uint32_t)n, (uint32_t)(n >> 32), block};
+    philox(c, k0, k1);
+    T* tag = nullptr;
+    T u1 = uniform_open(tag, c[0], c[1]);
+    T u2 = uniform_open(tag, c[2], c[3]);
+    T r = t_sqrt(mul_rn(T(-2), t_log(u1)));
+    T s, co;
+    t_sincos(mul_rn(mul_rn(T(2), t_pi(tag)), u2), &s, &co);
+    z1 = mul_rn(r, co);
+    z2 = mul_rn(r, s);
+}
+
+// ---------------------------------------------------------------- warps
+template <int L, class V>
+__device__ __forceinline__ V group_sum(V v) {
+#pragma unroll
+    for (int off = L / 2; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off, L);
+    return v;
+}
+template <int L>
+__device__ __forceinline__ int group_max(int v) {
+#pragma unroll
+    for (int off = L / 2; off > 0; off >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, off, L));
+    return v;
+}
+
+// ------------------------------------------------- coherent global loads
+// Data that other blocks write during the persistent kernel (records,
+// neighbour lists, flags, clocks, forces of the split step) is read at L2
+// (ld.global.cg), never through a possibly stale L1 line.
+__device__ __forceinline__ float ldcg(const float* p) { return __ldcg(p); }
+__device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
+__device__ __forceinline__ int ldcg(const int* p) { return __ldcg(p); }
+__device__ __forceinline__ long long ldcg(const long long* p) { return __ldcg(p); }
+__device__ __forceinline__ float4 ldcg(const float4* p) { return __ldcg(p); }
+__device__ __forceinline__ double2 ldcg(const double2* p) { return __ldcg(p); }
+
+// ------------------------------------------------------------ grid barrier
+// Barrier over all blocks of a cooperative launch (all co-resident).  Arrival
+// is an acq_rel atomic, the release a release store, the wait an acquire
+// load, so every write before the barrier is visible after it.  The last
+// block to arrive runs `last()` with all its threads before it releases the
+// others.  Waits are bounded: after SPIN_LIMIT polls a waiting block records
+// sync->error and the kernel returns (the host reports FCC_ERR_DEVICE)
+// instead of hanging.
+constexpr long long SPIN_LIMIT = 1ll << 22;  // ~0.1-4 s with the back-off below
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+template <class F>
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, F&& last) {
+    __shared__ int s_last, s_err;
+    __syncthreads();
+    unsigned gen = 0;
+    if (threadIdx.x == 0) {
+        gen = ld_acquire(&gs->gen);
+        unsigned prev = atom_add_acq_rel(&gs->count, 1u);
+        s_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        last();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            gs->count = 0;
+            __threadfence();
+            st_release(&gs->gen, gen + 1);
+        }
+    } else if (threadIdx.x == 0) {
+        long long it = 0;
+        while (ld_acquire(&gs->gen) == gen) {
+            if (++it > SPIN_LIMIT) {
+                atomicExch(&gs->error, 1);
+                break;
+            }
+            __nanosleep(32);
+        }
+    }
+    __syncthreads();
+    __threadfence();
+    if (threadIdx.x == 0) s_err = ld_acquire(&gs->error);
+    __syncthreads();
+    return s_err == 0;
+}
+
+}  // namespace fcc

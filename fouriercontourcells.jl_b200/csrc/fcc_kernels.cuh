@@ -1,0 +1,1073 @@
+// fcc_kernels.cuh — sm_100a kernels of the Fourier contour cell time step.
+//
+// One persistent cooperative kernel runs whole steps (k_step):
+//   [rebuild prologue, only when a simulation needs it: counting-sort cell
+//    list + neighbour list, five phases separated by grid barriers]
+//   forces + Euler-Maruyama update fused per body (no parent drag), or
+//   forces | barrier | displacement + update (parent drag: a body's motion
+//   needs its children's forces)
+//   grid barrier whose last block ticks the clocks and decides the next
+//   rebuild (the device-side form of update_neighbors!'s skin check).
+//
+// Work mapping of the force evaluation: L lanes per body (L = 8 for nθ = 40),
+// 32/L bodies per warp; lane l owns contour nodes k = l + L*s, s < S, so a
+// body's nθ nodes are spread evenly and node quadratures are L-lane shuffle
+// reductions.  Warp groups are the work units of a grid-stride loop.
+
+#pragma once
+
+#include "fcc_device.cuh"
+
+namespace fcc {
+
+// ---------------------------------------------------------- record access
+__device__ __forceinline__ void load_rec(const float* p, float (&r)[RECW]) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+    for (int u = 0; u < RECW / 4; ++u) {
+        float4 v = ldcg(q + u);
+        r[4 * u] = v.x;
+        r[4 * u + 1] = v.y;
+        r[4 * u + 2] = v.z;
+        r[4 * u + 3] = v.w;
+    }
+}
+__device__ __forceinline__ void load_rec(const double* p, double (&r)[RECW]) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+    for (int u = 0; u < RECW / 2; ++u) {
+        double2 v = ldcg(q + u);
+        r[2 * u] = v.x;
+        r[2 * u + 1] = v.y;
+    }
+}
+// x, y, rmax, w of a record
+__device__ __forceinline__ void load_head(const float* p, float& x, float& y, float& rm, float& w) {
+    float4 v = ldcg(reinterpret_cast<const float4*>(p));
+    x = v.x, y = v.y, rm = v.z, w = v.w;
+}
+__device__ __forceinline__ void load_head(const double* p, double& x, double& y, double& rm, double& w) {
+    double2 a = ldcg(reinterpret_cast<const double2*>(p));
+    double2 b = ldcg(reinterpret_cast<const double2*>(p) + 1);
+    x = a.x, y = a.y, rm = b.x, w = b.y;
+}
+// R0-scaled lab coefficients of a record (slots 4..22; slot 23 comes along)
+__device__ __forceinline__ void load_lab(const float* p, float (&c)[20]) {
+    const float4* q = reinterpret_cast<const float4*>(p + R_A0);
+#pragma unroll
+    for (int u = 0; u < 5; ++u) {
+        float4 v = ldcg(q + u);
+        c[4 * u] = v.x;
+        c[4 * u + 1] = v.y;
+        c[4 * u + 2] = v.z;
+        c[4 * u + 3] = v.w;
+    }
+}
+__device__ __forceinline__ void load_lab(const double* p, double (&c)[20]) {
+    const double2* q = reinterpret_cast<const double2*>(p + R_A0);
+#pragma unroll
+    for (int u = 0; u < 10; ++u) {
+        double2 v = ldcg(q + u);
+        c[2 * u] = v.x;
+        c[2 * u + 1] = v.y;
+    }
+}
+
+template <class T>
+__device__ __forceinline__ const T* rec_cur(const DevPtrs<T>& d, long long clk) {
+    return (clk & 1) ? d.rec1 : d.rec0;
+}
+template <class T>
+__device__ __forceinline__ T* rec_next(const DevPtrs<T>& d, long long clk) {
+    return (clk & 1) ? d.rec0 : d.rec1;
+}
+template <class T>
+__device__ __forceinline__ T* rec_cur_mut(const DevPtrs<T>& d, long long clk) {
+    return (clk & 1) ? d.rec1 : d.rec0;
+}
+
+__device__ __forceinline__ int jmod(int a, int n) {
+    int r = a % n;
+    return r < 0 ? r + n : r;
+}
+
+// grid coordinates, src/neighbors.jl:40-42 (clamped to the grid)
+template <class T>
+__device__ __forceinline__ void grid_coords(const SimDesc<T>& P, T x, T y, int& cx, int& cy) {
+    cx = max(0, min((int)div_rn(x, P.wx), P.ncx - 1));
+    cy = max(0, min((int)div_rn(y, P.wy), P.ncy - 1));
+}
+
+// ======================================================= rebuild phases ==
+// update_celllist! + update_neighbors! (src/neighbors.jl:81-92, 148-174,
+// 223-242) as a stable integer counting sort.  Each phase is a grid-stride
+// loop over the bodies or cells of the simulations flagged F_NEED.
+
+template <class T>
+__device__ void phase_count(const DevPtrs<T>& d, int tid, int nthr) {
+    for (int g = tid; g < d.Ntot; g += nthr) {
+        const int s = __ldg(d.sim_of + g);
+        if (!(ldcg(d.flags + s) & F_NEED)) continue;
+        const SimDesc<T>& P = d.sims[s];
+        const T* r = rec_cur(d, ldcg(d.clock + s)) + (size_t)g * RECW;
+        int cx, cy;
+        grid_coords(P, ldcg(r + R_X), ldcg(r + R_Y), cx, cy);
+        const int cell = P.cell_off + cx + P.ncx * cy;
+        d.cellid[g] = cell;
+        d.slot[g] = atomicAdd(&d.ccount[cell], 1);
+    }
+}
+
+// exclusive scan of the cell counts of each flagged simulation (one block per
+// simulation); cell c holds perm[cstart[c] .. cstop[c]).
+template <class T>
+__device__ void phase_scan(const DevPtrs<T>& d) {
+    __shared__ int s_warp[32];
+    __shared__ int s_carry;
+    const int nw = (blockDim.x + 31) / 32;
+    for (int s = blockIdx.x; s < d.nsims; s += gridDim.x) {
+        if (!(ldcg(d.flags + s) & F_NEED)) continue;
+        const SimDesc<T>& P = d.sims[s];
+        if (threadIdx.x == 0) s_carry = P.body_off;
+        __syncthreads();
+        for (int t0 = 0; t0 < P.ncells; t0 += blockDim.x) {
+            const int u = t0 + threadIdx.x;
+            const int c = P.cell_off + u;
+            const int v = u < P.ncells ? ldcg(d.ccount + c) : 0;
+            int incl = v;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                int o = __shfl_up_sync(0xffffffffu, incl, off);
+                if ((threadIdx.x & 31) >= off) incl += o;
+            }
+            if ((threadIdx.x & 31) == 31) s_warp[threadIdx.x >> 5] = incl;
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                int w = threadIdx.x < nw ? s_warp[threadIdx.x] : 0;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    int o = __shfl_up_sync(0xffffffffu, w, off);
+                    if ((int)threadIdx.x >= off) w += o;
+                }
+                s_warp[threadIdx.x] = w;  // inclusive over warps
+            }
+            __syncthreads();
+            const int carry = s_carry;
+            const int before = (threadIdx.x >> 5) ? s_warp[(threadIdx.x >> 5) - 1] : 0;
+            const int total = s_warp[nw - 1];
+            if (u < P.ncells) {
+                const int st = carry + before + incl - v;
+                d.cstart[c] = st;
+                d.cstop[c] = st + v;
+                d.ccount[c] = 0;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) s_carry = carry + total;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            d.builds[s] += 1;
+            d.maxcount[s] = 0;
+            atomicOr(&d.flags[s], F_VALID);
+        }
+        __syncthreads();
+    }
+}
+
+template <class T>
+__device__ void phase_scatter(const DevPtrs<T>& d, int tid, int nthr) {
+    for (int g = tid; g < d.Ntot; g += nthr) {
+        const int s = __ldg(d.sim_of + g);
+        if (!(ldcg(d.flags + s) & F_NEED)) continue;
+        d.perm[ldcg(d.cstart + ldcg(d.cellid + g)) + ldcg(d.slot + g)] = g;
+    }
+}
+
+// ties of the stable sortperm! (src/neighbors.jl:86) are ordered by body
+// index: sort each cell's few bodies ascending
+template <class T>
+__device__ void phase_sort(const DevPtrs<T>& d, int tid, int nthr) {
+    for (int c = tid; c < d.Ctot; c += nthr) {
+        const int s = __ldg(d.cell_sim + c);
+        if (!(ldcg(d.flags + s) & F_NEED)) continue;
+        const int a = ldcg(d.cstart + c), b = ldcg(d.cstop + c);
+        for (int q = a + 1; q < b; ++q) {
+            const int v = ldcg(d.perm + q);
+            int r = q - 1;
+            while (r >= a && ldcg(d.perm + r) > v) {
+                d.perm[r + 1] = ldcg(d.perm + r);
+                --r;
+            }
+            d.perm[r + 1] = v;
+        }
+    }
+}
+
+// neighbour list of one body: the 3x3 grid cells around it in the
+// reference's order (oy outer, ox inner), candidates in perm order, kept if
+// |ri - rj| <= rmax_i + rmax_j + range (exactly rounded like the oracle).
+template <class T>
+__device__ void phase_neighbors(const DevPtrs<T>& d, int tid, int nthr) {
+    for (int g = tid; g < d.Ntot; g += nthr) {
+        const int s = __ldg(d.sim_of + g);
+        if (!(ldcg(d.flags + s) & F_NEED)) continue;
+        const SimDesc<T>& P = d.sims[s];
+        const T* rc = rec_cur(d, ldcg(d.clock + s));
+        const T xi = ldcg(rc + (size_t)g * RECW + R_X), yi = ldcg(rc + (size_t)g * RECW + R_Y);
+        const T rmi = ldcg(rc + (size_t)g * RECW + R_RMAX);
+        const T ri = add_rn(rmi, P.nbrange);
+        int cx, cy;
+        grid_coords(P, xi, yi, cx, cy);
+        const int rx = P.ncx >= 3 ? 1 : 0, ry = P.ncy >= 3 ? 1 : 0;
+        int n = 0;
+        int* out = d.nb_idx + (size_t)g * d.cap;
+        for (int oy = -ry; oy <= ry; ++oy)
+            for (int ox = -rx; ox <= rx; ++ox) {
+                const int cell = P.cell_off + jmod(cx + ox, P.ncx) + P.ncx * jmod(cy + oy, P.ncy);
+                const int qa = ldcg(d.cstart + cell), qb = ldcg(d.cstop + cell);
+                for (int q = qa; q < qb; ++q) {
+                    const int j = ldcg(d.perm + q);
+                    if (j == g) continue;
+                    const T xj = ldcg(rc + (size_t)j * RECW + R_X), yj = ldcg(rc + (size_t)j * RECW + R_Y);
+                    const T rmj = ldcg(rc + (size_t)j * RECW + R_RMAX);
+                    const T dx = minimum_image_exact(sub_rn(xi, xj), P.Lx);
+                    const T dy = minimum_image_exact(sub_rn(yi, yj), P.Ly);
+                    const T lim = add_rn(ri, rmj);
+                    if (add_rn(mul_rn(dx, dx), mul_rn(dy, dy)) <= mul_rn(lim, lim)) {
+                        ++n;
+                        if (n <= d.cap) out[n - 1] = j;
+                    }
+                }
+            }
+        d.nb_count[g] = n;
+        if (n > d.cap) atomicOr(&d.flags[s], F_FROZEN);
+        atomicMax(&d.maxcount[s], n);
+        if (P.skin > T(0)) {
+            d.x0[g] = xi;
+            d.y0[g] = yi;
+            d.rmax0[g] = rmi;
+        }
+    }
+}
+
+// ============================================================= update ==
+// Translational displacement of a body with substrate drag, plus the forces
+// of its children with parent drag (src/dynamics.jl:84-99).
+template <class T>
+__device__ __forceinline__ void substrate_displacement(const DevPtrs<T>& d, const SimDesc<T>& P, const T* rc, int c,
+                                                       long long clk, T& ox, T& oy) {
+    const int tc = unpack_w(ldcg(rc + (size_t)c * RECW + R_W)) & 7;
+    T fx = ldcg(d.gx + c), fy = ldcg(d.gy + c);
+    const int nch = __ldg(d.ch_count + c);
+    for (int q = 0; q < nch; ++q) {
+        const int k = __ldg(d.ch_idx + (size_t)c * d.ccap + q);
+        const int tk = unpack_w(ldcg(rc + (size_t)k * RECW + R_W)) & 7;
+        if (P.parent_drag[tk]) {
+            fx += ldcg(d.gx + k);
+            fy += ldcg(d.gy + k);
+        }
+    }
+    T so, co;
+    t_sincos(ldcg(rc + (size_t)c * RECW + R_TH), &so, &co);
+    const T dt = P.dt;
+    const T sig = t_sqrt(T(2) * P.Dt[tc] * dt);
+    T x1 = T(0), x2 = T(0);
+    if (sig != T(0)) philox_pair<T>(P.k0, P.k1, (uint32_t)(c - P.body_off + 1), (uint64_t)clk, 0u, x1, x2);
+    ox = dt * (P.v0[tc] * co - P.mur[tc] * fx) + sig * x1;
+    oy = dt * (P.v0[tc] * so - P.mur[tc] * fy) + sig * x2;
+}
+
+// Euler-Maruyama update of body g by the L lanes of its group
+// (src/dynamics.jl:128-203 with frame = true): body-frame gradient, theta and
+// shape update, shape bound projection and a0 (FP64 accumulation), wrap,
+// lab frame of the new state into rec[next], skin check.  fx, fy, tt and gl
+// are the group-reduced gradients (uniform across the group).
+template <class T, int L>
+__device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T>& P, bool act, int g, int s, int l,
+                                            long long clk, const T (&rv)[RECW], T r0, int ti, T fx, T fy, T tt,
+                                            const T (&gl)[NCM], bool split) {
+    constexpr unsigned FULL = 0xffffffffu;
+    constexpr int MPL = (KM + L - 1) / L;
+    const T dt = P.dt;
+    const T tho = rv[R_TH];
+    const uint32_t li = (uint32_t)(g - P.body_off + 1);
+    const T sig_r = t_sqrt(T(2) * P.Dr[ti] * dt);
+    T z3 = T(0);
+    if (act && l == 0 && sig_r != T(0)) {
+        T z4;
+        philox_pair<T>(P.k0, P.k1, li, (uint64_t)clk, 1u, z3, z4);
+    }
+    z3 = __shfl_sync(FULL, z3, 0, L);
+    const T thn = tho - (dt * P.muth[ti]) * tt + sig_r * z3;
+
+    T* cf = d.coef + (size_t)(act ? g : 0) * NCM;
+    const T a0 = ldcg(cf);
+    const T ga0 = r0 * gl[0];
+    const T dtmu = dt * P.muab[ti];
+    const int K = P.K;
+    T an[MPL], bn[MPL];
+    double sp = 0.0;
+#pragma unroll
+    for (int u = 0; u < MPL; ++u) {
+        const int m = l + u * L;
+        an[u] = T(0);
+        bn[u] = T(0);
+        if (m < K) {
+            T ga = gl[1], gb = gl[1 + KM];
+#pragma unroll
+            for (int mm = 1; mm < KM; ++mm)
+                if (mm == m) ga = gl[1 + mm], gb = gl[1 + KM + mm];
+            ga *= r0;
+            gb *= r0;
+            T so, co;
+            t_sincos(T(m + 2) * tho, &so, &co);
+            const T a = ldcg(cf + 1 + m), b = ldcg(cf + 1 + KM + m);
+            const T gca = ga * co + gb * so - ga0 * a / (T(2) * a0);
+            const T gcb = -ga * so + gb * co - ga0 * b / (T(2) * a0);
+            an[u] = a - dtmu * gca;
+            bn[u] = b - dtmu * gcb;
+            sp += sqrt((double)an[u] * (double)an[u] + (double)bn[u] * (double)bn[u]);
+        }
+    }
+    // enforce_shape! (src/dynamics.jl:44-64) with FP64 sums
+    const double ssum = group_sum<L>(sp);
+    if (ssum > SHAPE_BOUND) {
+        const double f = SHAPE_BOUND / ssum;
+#pragma unroll
+        for (int u = 0; u < MPL; ++u) {
+            an[u] = T((double)an[u] * f);
+            bn[u] = T((double)bn[u] * f);
+        }
+    }
+    double qp = 0.0;
+#pragma unroll
+    for (int u = 0; u < MPL; ++u) qp += (double)an[u] * (double)an[u] + (double)bn[u] * (double)bn[u];
+    const double qs = group_sum<L>(qp);
+    const T a0n = T(sqrt(1.0 - qs * 0.5));
+
+    // lab frame of the new state (src/geometry.jl:208-227)
+    T* rn = rec_next(d, clk) + (size_t)(act ? g : 0) * RECW;
+    T bp = T(0);
+#pragma unroll
+    for (int u = 0; u < MPL; ++u) {
+        const int m = l + u * L;
+        if (m < K) {
+            T so, co;
+            t_sincos(T(m + 2) * thn, &so, &co);
+            const T al = an[u] * co - bn[u] * so;
+            const T be = an[u] * so + bn[u] * co;
+            bp += t_sqrt(an[u] * an[u] + bn[u] * bn[u]);
+            if (act) {
+                rn[R_AL + m] = r0 * al;
+                rn[R_BE + m] = r0 * be;
+                cf[1 + m] = an[u];
+                cf[1 + KM + m] = bn[u];
+            }
+        }
+    }
+    const T rmax = r0 * (a0n + group_sum<L>(bp));
+
+    if (act && l == 0) {
+        T dxp, dyp;
+        if (split) {
+            const T* rc = rec_cur(d, clk);
+            if (P.parent_drag[ti]) {
+                const int c = unpack_w(rv[R_W]) >> 3;
+                T ux, uy;
+                substrate_displacement(d, P, rc, c, clk, ux, uy);
+                T so, co;
+                t_sincos(tho, &so, &co);
+                const T sig = t_sqrt(T(2) * P.Dt[ti] * dt);
+                T x1 = T(0), x2 = T(0);
+                if (sig != T(0)) philox_pair<T>(P.k0, P.k1, li, (uint64_t)clk, 0u, x1, x2);
+                dxp = ux + dt * (P.v0[ti] * co - P.mur[ti] * fx) + sig * x1;
+                dyp = uy + dt * (P.v0[ti] * so - P.mur[ti] * fy) + sig * x2;
+            } else {
+                substrate_displacement(d, P, rc, g, clk, dxp, dyp);
+            }
+        } else {
+            T so, co;
+            t_sincos(tho, &so, &co);
+            const T sig = t_sqrt(T(2) * P.Dt[ti] * dt);
+            T x1 = T(0), x2 = T(0);
+            if (sig != T(0)) philox_pair<T>(P.k0, P.k1, li, (uint64_t)clk, 0u, x1, x2);
+            dxp = dt * (P.v0[ti] * co - P.mur[ti] * fx) + sig * x1;
+            dyp = dt * (P.v0[ti] * so - P.mur[ti] * fy) + sig * x2;
+        }
+        int sx, sy;
+        const T xw = wrap_exact(add_rn(rv[R_X], dxp), P.Lx, sx);
+        const T yw = wrap_exact(add_rn(rv[R_Y], dyp), P.Ly, sy);
+        d.imgx[g] += sx;
+        d.imgy[g] += sy;
+        rn[R_X] = xw;
+        rn[R_Y] = yw;
+        rn[R_RMAX] = rmax;
+        rn[R_W] = rv[R_W];
+        rn[R_A0] = r0 * a0n;
+        rn[R_TH] = thn;
+        cf[0] = a0n;
+        const int f = ldcg(d.flags + s);
+        // skin check of the new state (src/neighbors.jl:198-205)
+        if ((f & F_CONTACT) && (f & F_VALID) && P.skin > T(0)) {
+            const T dx = minimum_image_exact(sub_rn(xw, ldcg(d.x0 + g)), P.Lx);
+            const T dy = minimum_image_exact(sub_rn(yw, ldcg(d.y0 + g)), P.Ly);
+            const T grow = sub_rn(rmax, ldcg(d.rmax0 + g));
+            const T delta = add_rn(t_sqrt(add_rn(mul_rn(dx, dx), mul_rn(dy, dy))), grow > T(0) ? grow : T(0));
+            if (mul_rn(T(2), delta) > P.skin) atomicOr(&d.flags[s], F_REBUILD);
+        }
+        if (!(isfinite(xw) && isfinite(yw) && isfinite(thn) && isfinite(rmax))) atomicOr(&d.flags[s], F_NONFINITE);
+    }
+}
+
+// ==================================================== force evaluation ==
+enum : int { MODE_FUSED = 0, MODE_FORCES = 1, MODE_DIAG = 2 };
+
+// Forces on the 32/L bodies of warp group `wg`, and in MODE_FUSED their
+// update.  Follows, per body i:
+//   contour synthesis R, R' at the nodes        src/geometry.jl:248-257
+//   body terms (Tension, PerimeterElasticity)   src/gradients.jl:70-98, 197-228
+//   contact pressure at the nodes (Overlap,     src/energies/contact.jl:300-324,
+//     LinearRepulsion) and its gradients          391-429; src/gradients.jl:265-307
+//   bond forces                                 src/energies/bonds.jl:98-111
+//   pullback glab = S' Gall                     src/gradients.jl:374-386
+template <class T, int L, int S, bool ONE, int MODE>
+__device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg) {
+    constexpr int BPW = 32 / L;
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int l = lane & (L - 1);
+    const int g = wg * BPW + lane / L;
+    bool act = g < d.Ntot;
+    const int s = act ? __ldg(d.sim_of + g) : 0;
+    const int fl = ldcg(d.flags + s);
+    if (MODE != MODE_DIAG) act = act && (fl & F_ACTIVE) && !(fl & F_FROZEN);
+    const int gg = act ? g : 0;
+    const SimDesc<T>& P = d.sims[s];
+    const long long clk = ldcg(d.clock + s);
+    const T* rc = rec_cur(d, clk);
+    const int nth = P.nth;
+    const T dphi = P.dphi;
+
+    T rv[RECW];
+    load_rec(rc + (size_t)gg * RECW, rv);
+    const int wv = unpack_w(rv[R_W]);
+    const int ti = wv & 7;
+    const int pi = wv >> 3;
+    const T r0 = __ldg(d.R0 + gg);
+
+    T R[S], R1[S], C1[S], S1[S];
+    unsigned vmask = 0;
+    const int nch = ONE ? 1 : (nth + L * S - 1) / (L * S);
+
+    auto synth = [&](int ch) {
+        vmask = 0;
+#pragma unroll
+        for (int sl = 0; sl < S; ++sl) {
+            const int k = ch * L * S + l + L * sl;
+            const bool v = k < nth;
+            const T c1 = v ? __ldg(d.cs + 2 * k) : T(1);
+            const T s1 = v ? __ldg(d.cs + 2 * k + 1) : T(0);
+            C1[sl] = c1;
+            S1[sl] = s1;
+            T c = c1, sn = s1, r = rv[R_A0], r1 = T(0);
+#pragma unroll
+            for (int m = 0; m < KM; ++m) {
+                const T n = T(m + 2);
+                const T cn = c * c1 - sn * s1;
+                sn = sn * c1 + c * s1;
+                c = cn;
+                const T al = rv[R_AL + m], be = rv[R_BE + m];
+                r += al * c + be * sn;
+                r1 += n * (be * c - al * sn);
+            }
+            R[sl] = v ? r : T(0);
+            R1[sl] = v ? r1 : T(0);
+            if (v) vmask |= 1u << sl;
+        }
+    };
+
+    // ---- pass 1: contour integral Q = sum_k sqrt(R^2 + R'^2) dphi
+    T Qp = T(0);
+    for (int ch = 0; ch < nch; ++ch) {
+        synth(ch);
+#pragma unroll
+        for (int sl = 0; sl < S; ++sl)
+            if (vmask & (1u << sl)) Qp += t_sqrt(R[sl] * R[sl] + R1[sl] * R1[sl]);
+    }
+    const T Q = group_sum<L>(Qp) * dphi;
+
+    // ---- body terms: W = sum_t dF_t/dQ * dphi, E = e_1 + (e_2 + ...)
+    T W = T(0), E = T(0);
+    {
+        const int nbt = P.nbt;
+        for (int q = 0; q < nbt; ++q) {
+            if (!(P.bt_mask[q] & (1u << ti))) continue;
+            const T a = P.bt_a[q];
+            W += P.bt_kind[q] == BT_TENSION ? a : a * (T(2) * (Q - P.bt_b[q] * r0));
+        }
+        for (int q = nbt - 1; q >= 0; --q) {
+            if (!(P.bt_mask[q] & (1u << ti))) continue;
+            const T a = P.bt_a[q];
+            const T dq = Q - P.bt_b[q] * r0;
+            E = (P.bt_kind[q] == BT_TENSION ? a * Q : a * (dq * dq)) + E;
+        }
+        W *= dphi;
+    }
+
+    // ---- pass 2: contact pressure, contour gradients, force/torque and pullback partials
+    T fx = T(0), fy = T(0), tt = T(0);
+    T gl[NCM];
+#pragma unroll
+    for (int r = 0; r < NCM; ++r) gl[r] = T(0);
+
+    const bool contact = act && (fl & F_CONTACT);
+    const int cnt = contact ? min(ldcg(d.nb_count + gg), d.cap) : 0;
+    const int maxc = __reduce_max_sync(FULL, cnt);
+    const T xi = rv[R_X], yi = rv[R_Y];
+    const T Lx = P.Lx, Ly = P.Ly, iLx = P.invLx, iLy = P.invLy, crange = P.crange;
+    const bool rewrap = P.rewrap != 0;
+
+    for (int ch = 0; ch < nch; ++ch) {
+        if (!ONE) synth(ch);
+        T p[S];
+#pragma unroll
+        for (int sl = 0; sl < S; ++sl) p[sl] = T(0);
+        if (maxc > 0) {
+            T rcx[S], rcy[S];
+#pragma unroll
+            for (int sl = 0; sl < S; ++sl) {
+                rcx[sl] = R[sl] * C1[sl];
+                rcy[sl] = R[sl] * S1[sl];
+            }
+            for (int q = 0; q < maxc; ++q) {
+                const bool qa = q < cnt;
+                const int j = qa ? ldcg(d.nb_idx + (size_t)gg * d.cap + q) : gg;
+                T xj, yj, rmj, wj;
+                load_head(rc + (size_t)j * RECW, xj, yj, rmj, wj);
+                const T dxc = minimum_image_fast(xi - xj, Lx, iLx);
+                const T dyc = minimum_image_fast(yi - yj, Ly, iLy);
+                const T lim = rmj + crange;
+                const T lim2 = lim * lim;
+                unsigned hm = 0;
+                if (qa) {
+#pragma unroll
+                    for (int sl = 0; sl < S; ++sl) {
+                        T dx = rcx[sl] + dxc, dy = rcy[sl] + dyc;
+                        if (rewrap) {
+                            dx = minimum_image_fast(dx, Lx, iLx);
+                            dy = minimum_image_fast(dy, Ly, iLy);
+                        }
+                        if ((vmask & (1u << sl)) && dx * dx + dy * dy <= lim2) hm |= 1u << sl;
+                    }
+                }
+                // one hit per lane per round: the hit path runs as many rounds as
+                // the busiest lane has hits for this neighbour (usually one)
+                while (__any_sync(FULL, hm != 0)) {
+                    if (hm) {
+                        const int sl = __ffs(hm) - 1;
+                        hm &= hm - 1;
+                        T rx = rcx[0], ry = rcy[0];
+#pragma unroll
+                        for (int u = 1; u < S; ++u)
+                            if (sl == u) rx = rcx[u], ry = rcy[u];
+                        T dx = rx + dxc, dy = ry + dyc;
+                        if (rewrap) {
+                            dx = minimum_image_fast(dx, Lx, iLx);
+                            dy = minimum_image_fast(dy, Ly, iLy);
+                        }
+                        const T dist = t_sqrt(dx * dx + dy * dy);
+                        T cp = T(1), sp = T(0);
+                        if (dist > T(0)) {
+                            const T inv = T(1) / dist;
+                            cp = dx * inv;
+                            sp = dy * inv;
+                        }
+                        T lj[20];
+                        load_lab(rc + (size_t)j * RECW, lj);
+                        // R_j(psi) by the angle-addition recurrence (src/geometry.jl:282-291)
+                        T c = cp, sn = sp, rj = lj[0];
+#pragma unroll
+                        for (int m = 0; m < KM; ++m) {
+                            const T cn = c * cp - sn * sp;
+                            sn = sn * cp + c * sp;
+                            c = cn;
+                            rj += lj[1 + m] * c + lj[1 + KM + m] * sn;
+                        }
+                        const T dd = rj - dist;
+                        const int wjv = unpack_w(wj);
+                        const int tj = wjv & 7;
+                        const int rel = (wjv >> 3) == pi ? 1 : 0;
+                        T gv = dd >= T(0) ? P.cA[rel][ti][tj] : T(0);
+                        if (dd > T(0)) gv += P.cB[ti] * dd;
+#pragma unroll
+                        for (int u = 0; u < S; ++u)
+                            if (sl == u) p[u] += gv;
+                    }
+                }
+            }
+        }
+        // contour gradients of node k: GR = W R/q + p dphi R, GD = W R'/q, GDD = 0
+#pragma unroll
+        for (int sl = 0; sl < S; ++sl) {
+            if (!(vmask & (1u << sl))) continue;
+            const T r = R[sl], r1 = R1[sl], c1 = C1[sl], s1 = S1[sl];
+            const T q = t_sqrt(r * r + r1 * r1);
+            const T iq = T(1) / q;
+            const T pw = p[sl] * dphi;
+            const T GRk = W * r * iq + pw * r;
+            const T GDk = W * r1 * iq;
+            fx += pw * (r * c1 + r1 * s1);
+            fy += pw * (r * s1 - r1 * c1);
+            tt += (-pw * r) * r1;
+            gl[0] += GRk;
+            T c = c1, sn = s1;
+#pragma unroll
+            for (int m = 0; m < KM; ++m) {
+                const T n = T(m + 2);
+                const T cn = c * c1 - sn * s1;
+                sn = sn * c1 + c * s1;
+                c = cn;
+                gl[1 + m] += c * GRk - n * sn * GDk;
+                gl[1 + KM + m] += sn * GRk + n * c * GDk;
+            }
+            if (MODE == MODE_DIAG && act) {
+                const int k = ch * L * S + l + L * sl;
+                const size_t o = (size_t)g * nth + k;
+                d.P[o] = p[sl];
+                d.GR[o] = GRk;
+                d.GD[o] = GDk;
+                d.GDD[o] = T(0);
+            }
+        }
+    }
+
+    fx = group_sum<L>(fx);
+    fy = group_sum<L>(fy);
+    tt = group_sum<L>(tt);
+#pragma unroll
+    for (int r = 0; r < NCM; ++r) gl[r] = group_sum<L>(gl[r]);
+
+    // ---- bond forces on the centre (every lane of the body, no shuffles)
+    if (act && P.nbd > 0) {
+        const int bc = __ldg(d.bd_count + g);
+        T bx = T(0), by = T(0);
+        for (int q = 0; q < bc; ++q) {
+            const int j = __ldg(d.bd_idx + (size_t)g * d.bcap + q);
+            T xj, yj, rmj, wj;
+            load_head(rc + (size_t)j * RECW, xj, yj, rmj, wj);
+            const int tj = unpack_w(wj) & 7;
+            const T d0 = minimum_image_exact(sub_rn(xi, xj), Lx);
+            const T d1 = minimum_image_exact(sub_rn(yi, yj), Ly);
+            T a0 = T(0), a1 = T(0);
+            for (int u = P.nbd - 1; u >= 0; --u) {
+                const uint32_t mk = P.bd_mask[u];
+                if (!((mk >> ti) & 1u) || !((mk >> tj) & 1u)) continue;
+                const T rr = t_sqrt(d0 * d0 + d1 * d1);
+                const T k = P.bd_k[u], rb = P.bd_r0[u];
+                const T f = rr > T(0) ? k * (T(1) - rb / rr) : (rb == T(0) ? k : T(0));
+                a0 = f * d0 + a0;
+                a1 = f * d1 + a1;
+            }
+            bx += a0;
+            by += a1;
+        }
+        fx += bx;
+        fy += by;
+    }
+
+    if (MODE == MODE_FORCES || MODE == MODE_DIAG) {
+        if (act) {
+            if (l == 0) {
+                d.gx[g] = fx;
+                d.gy[g] = fy;
+                d.gth[g] = tt;
+                d.E[g] = E;
+            }
+#pragma unroll
+            for (int r = 0; r < NCM; ++r)
+                if ((r & (L - 1)) == l) d.glab[(size_t)g * NCM + r] = gl[r];
+        }
+        if (MODE == MODE_DIAG && act) {
+            // body-frame gradient gcoef (src/gradients.jl:347-362), frame = true
+            const T* cf = d.coef + (size_t)g * NCM;
+            const T a0 = ldcg(cf);
+            const T ga0 = r0 * gl[0];
+            const T tho = rv[R_TH];
+#pragma unroll
+            for (int u = 0; u < (KM + L - 1) / L; ++u) {
+                const int m = l + u * L;
+                if (m >= P.K) continue;
+                T ga = gl[1], gb = gl[1 + KM];
+#pragma unroll
+                for (int mm = 1; mm < KM; ++mm)
+                    if (mm == m) ga = gl[1 + mm], gb = gl[1 + KM + mm];
+                ga *= r0;
+                gb *= r0;
+                T so, co;
+                t_sincos(T(m + 2) * tho, &so, &co);
+                const T a = ldcg(cf + 1 + m), b = ldcg(cf + 1 + KM + m);
+                d.gcoef[(size_t)g * NCM + 1 + m] = ga * co + gb * so - ga0 * a / (T(2) * a0);
+                d.gcoef[(size_t)g * NCM + 1 + KM + m] = -ga * so + gb * co - ga0 * b / (T(2) * a0);
+            }
+            if (l == 0) d.gcoef[(size_t)g * NCM] = ga0;
+        }
+        return;
+    }
+
+    // the last step's centre gradients and body energy stay readable, as the
+    // reference's sim.grad does after step!
+    if (act && l == 0) {
+        d.gx[g] = fx;
+        d.gy[g] = fy;
+        d.gth[g] = tt;
+        d.E[g] = E;
+    }
+    update_body<T, L>(d, P, act, g, s, l, clk, rv, r0, ti, fx, fy, tt, gl, false);
+}
+
+// Phase B of the split step: displacement with parent drag + update of the
+// bodies of warp group `wg`, from the forces phase A stored.
+template <class T, int L>
+__device__ __forceinline__ void update_warp_split(const DevPtrs<T>& d, int wg) {
+    constexpr int BPW = 32 / L;
+    const int lane = threadIdx.x & 31;
+    const int l = lane & (L - 1);
+    const int g = wg * BPW + lane / L;
+    bool act = g < d.Ntot;
+    const int s = act ? __ldg(d.sim_of + g) : 0;
+    const int fl = ldcg(d.flags + s);
+    act = act && (fl & F_ACTIVE) && !(fl & F_FROZEN);
+    const int gg = act ? g : 0;
+    const SimDesc<T>& P = d.sims[s];
+    const long long clk = ldcg(d.clock + s);
+    T rv[RECW];
+    load_rec(rec_cur(d, clk) + (size_t)gg * RECW, rv);
+    const int ti = unpack_w(rv[R_W]) & 7;
+    const T r0 = __ldg(d.R0 + gg);
+    T gl[NCM];
+#pragma unroll
+    for (int r = 0; r < NCM; ++r) gl[r] = ldcg(d.glab + (size_t)gg * NCM + r);
+    const T fx = ldcg(d.gx + gg), fy = ldcg(d.gy + gg), tt = ldcg(d.gth + gg);
+    update_body<T, L>(d, P, act, g, s, l, clk, rv, r0, ti, fx, fy, tt, gl, true);
+}
+
+// Last block of a step's closing barrier: tick the clocks of the simulations
+// that stepped and decide the rebuilds of the next step (skin exceeded, list
+// invalid, or skin = 0: src/simulation.jl:132-142).
+template <class T>
+__device__ void bookkeeping(const DevPtrs<T>& d) {
+    __shared__ int s_any;
+    if (threadIdx.x == 0) s_any = 0;
+    __syncthreads();
+    for (int s = threadIdx.x; s < d.nsims; s += blockDim.x) {
+        int f = ldcg(d.flags + s);
+        if ((f & F_ACTIVE) && !(f & F_FROZEN)) {
+            d.clock[s] = ldcg(d.clock + s) + 1;
+            const bool need = (f & F_CONTACT) && ((f & F_REBUILD) || !(f & F_VALID) || d.sims[s].skin == T(0));
+            f &= ~(F_REBUILD | F_NEED);
+            if (need) {
+                f |= F_NEED;
+                s_any = 1;
+            }
+        } else {
+            f &= ~F_NEED;
+        }
+        d.flags[s] = f;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) d.sync->any_need = s_any;
+}
+
+// ============================================================= kernels ==
+template <class T>
+__device__ __forceinline__ bool rebuild_prologue(const DevPtrs<T>& d, int tid, int nthr) {
+    auto noop = [] {};
+    phase_count(d, tid, nthr);
+    if (!grid_barrier(d.sync, noop)) return false;
+    phase_scan(d);
+    if (!grid_barrier(d.sync, noop)) return false;
+    phase_scatter(d, tid, nthr);
+    if (!grid_barrier(d.sync, noop)) return false;
+    phase_sort(d, tid, nthr);
+    if (!grid_barrier(d.sync, noop)) return false;
+    phase_neighbors(d, tid, nthr);
+    return grid_barrier(d.sync, noop);
+}
+
+// Persistent cooperative step kernel: `nsteps` whole time steps per launch.
+template <class T, int L, int S, bool ONE, bool SPLIT>
+__global__ void __launch_bounds__(256) k_step(DevPtrs<T> d, int nsteps) {
+    const int wpb = blockDim.x >> 5;
+    const int wid = blockIdx.x * wpb + (threadIdx.x >> 5);
+    const int nwarps = gridDim.x * wpb;
+    const int ngroups = (d.Ntot + (32 / L) - 1) / (32 / L);
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nthr = gridDim.x * blockDim.x;
+    for (int st = 0; st < nsteps; ++st) {
+        if (ld_acquire(&d.sync->any_need))
+            if (!rebuild_prologue(d, tid, nthr)) return;
+        for (int wg = wid; wg < ngroups; wg += nwarps)
+            forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg);
+        if (SPLIT) {
+            if (!grid_barrier(d.sync, [] {})) return;
+            for (int wg = wid; wg < ngroups; wg += nwarps) update_warp_split<T, L>(d, wg);
+        }
+        if (!grid_barrier(d.sync, [&] { bookkeeping(d); })) return;
+    }
+}
+
+// compute_gradients! (src/simulation.jl:150-158): forces and every gradient
+// buffer of the current state, no update.
+template <class T, int L, int S, bool ONE>
+__global__ void __launch_bounds__(256) k_gradients(DevPtrs<T> d) {
+    const int wpb = blockDim.x >> 5;
+    const int wg = blockIdx.x * wpb + (threadIdx.x >> 5);
+    const int ngroups = (d.Ntot + (32 / L) - 1) / (32 / L);
+    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG>(d, wg);
+}
+
+// Stand-alone rebuild phases (update_neighbors!, and the stateless neighbour
+// build), one launch per phase.
+template <class T>
+__global__ void k_phase_count(DevPtrs<T> d) {
+    if (ldcg(&d.sync->any_need)) phase_count(d, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+template <class T>
+__global__ void k_phase_scan(DevPtrs<T> d) {
+    if (ldcg(&d.sync->any_need)) phase_scan(d);
+}
+template <class T>
+__global__ void k_phase_scatter(DevPtrs<T> d) {
+    if (ldcg(&d.sync->any_need)) phase_scatter(d, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+template <class T>
+__global__ void k_phase_sort(DevPtrs<T> d) {
+    if (ldcg(&d.sync->any_need)) phase_sort(d, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+template <class T>
+__global__ void k_phase_neighbors(DevPtrs<T> d) {
+    if (ldcg(&d.sync->any_need)) phase_neighbors(d, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+// Skin check of the current state (skin_check_kernel!, src/neighbors.jl:188-194).
+template <class T>
+__global__ void k_skin_check(DevPtrs<T> d) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= d.Ntot) return;
+    const int s = __ldg(d.sim_of + g);
+    const int f = ldcg(d.flags + s);
+    if (!(f & F_CONTACT) || !(f & F_VALID)) return;
+    const SimDesc<T>& P = d.sims[s];
+    if (!(P.skin > T(0))) return;
+    const T* r = rec_cur(d, ldcg(d.clock + s)) + (size_t)g * RECW;
+    const T dx = minimum_image_exact(sub_rn(ldcg(r + R_X), ldcg(d.x0 + g)), P.Lx);
+    const T dy = minimum_image_exact(sub_rn(ldcg(r + R_Y), ldcg(d.y0 + g)), P.Ly);
+    const T grow = sub_rn(ldcg(r + R_RMAX), ldcg(d.rmax0 + g));
+    const T delta = add_rn(t_sqrt(add_rn(mul_rn(dx, dx), mul_rn(dy, dy))), grow > T(0) ? grow : T(0));
+    if (mul_rn(T(2), delta) > P.skin) atomicOr(&d.flags[s], F_REBUILD);
+}
+
+// Decide which simulations rebuild in the stand-alone update_neighbors!.
+template <class T>
+__global__ void k_prepare_rebuild(DevPtrs<T> d, int force) {
+    __shared__ int s_any;
+    if (threadIdx.x == 0) s_any = 0;
+    __syncthreads();
+    for (int s = threadIdx.x; s < d.nsims; s += blockDim.x) {
+        int f = d.flags[s];
+        const bool need = (f & F_ACTIVE) && (f & F_CONTACT) &&
+                          (force || (f & F_REBUILD) || !(f & F_VALID) || d.sims[s].skin == T(0));
+        f &= ~(F_REBUILD | F_NEED);
+        if (need) {
+            f |= F_NEED;
+            s_any = 1;
+        }
+        d.flags[s] = f;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) d.sync->any_need = s_any;
+}
+
+// After a stand-alone rebuild: the next step rebuilds again only with skin = 0.
+template <class T>
+__global__ void k_finish_rebuild(DevPtrs<T> d) {
+    for (int s = threadIdx.x; s < d.nsims; s += blockDim.x) {
+        int f = d.flags[s];
+        const bool need = (f & F_ACTIVE) && (f & F_CONTACT) && !(f & F_FROZEN) && d.sims[s].skin == T(0);
+        f &= ~(F_REBUILD | F_NEED);
+        if (need) f |= F_NEED;
+        d.flags[s] = f;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int any = 0;
+        for (int s = 0; s < d.nsims; ++s) any |= (d.flags[s] & F_NEED) ? 1 : 0;
+        d.sync->any_need = any;
+    }
+}
+
+// Simulation set-up and set_state: enforce_shape! (FP64 sums) and the lab
+// frame of the given body state into rec[clock & 1] (src/simulation.jl:102-103,
+// src/dynamics.jl:44-64, src/geometry.jl:208-227).  One thread per body.
+template <class T>
+__global__ void k_init(DevPtrs<T> d, const T* __restrict__ x, const T* __restrict__ y, const T* __restrict__ th,
+                       const T* __restrict__ coef_in) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= d.Ntot) return;
+    const int s = d.sim_of[g];
+    const SimDesc<T>& P = d.sims[s];
+    const int K = P.K;
+    T c[NCM];
+#pragma unroll
+    for (int r = 0; r < NCM; ++r) c[r] = coef_in[(size_t)g * NCM + r];
+    double ssum = 0.0;
+    for (int m = 0; m < K; ++m) ssum += sqrt((double)c[1 + m] * c[1 + m] + (double)c[1 + KM + m] * c[1 + KM + m]);
+    if (ssum > SHAPE_BOUND) {
+        const double f = SHAPE_BOUND / ssum;
+        for (int m = 0; m < K; ++m) {
+            c[1 + m] = T((double)c[1 + m] * f);
+            c[1 + KM + m] = T((double)c[1 + KM + m] * f);
+        }
+    }
+    double q = 0.0;
+    for (int m = 0; m < K; ++m) q += (double)c[1 + m] * c[1 + m] + (double)c[1 + KM + m] * c[1 + KM + m];
+    c[0] = T(sqrt(1.0 - q * 0.5));
+    const T r0 = d.R0[g];
+    T* rn = rec_cur_mut(d, d.clock[s]) + (size_t)g * RECW;
+    T* ro = rec_next(d, d.clock[s]) + (size_t)g * RECW;
+    T bound = c[0];
+    for (int r = 0; r < RECW; ++r) ro[r] = T(0);
+    for (int m = 0; m < KM; ++m) {
+        T al = T(0), be = T(0);
+        if (m < K) {
+            T so, co;
+            t_sincos(T(m + 2) * th[g], &so, &co);
+            al = c[1 + m] * co - c[1 + KM + m] * so;
+            be = c[1 + m] * so + c[1 + KM + m] * co;
+            bound += t_sqrt(c[1 + m] * c[1 + m] + c[1 + KM + m] * c[1 + KM + m]);
+        }
+        rn[R_AL + m] = r0 * al;
+        rn[R_BE + m] = r0 * be;
+    }
+    rn[R_X] = x[g];
+    rn[R_Y] = y[g];
+    rn[R_RMAX] = r0 * bound;
+    rn[R_A0] = r0 * c[0];  // R_W (parent, type) is written by k_set_w
+    rn[R_TH] = th[g];
+#pragma unroll
+    for (int r = 0; r < NCM; ++r) d.coef[(size_t)g * NCM + r] = c[r];
+}
+
+// w field (parent, type) of the current record
+template <class T>
+__global__ void k_set_w(DevPtrs<T> d, const int* __restrict__ w) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= d.Ntot) return;
+    T* tag = nullptr;
+    rec_cur_mut(d, d.clock[d.sim_of[g]])[(size_t)g * RECW + R_W] = pack_w(w[g], tag);
+}
+
+// Geometry of the current state for get_geometry: lab, labR0, rmax, and
+// R, R', R'' at the nodes (src/geometry.jl:13-32, 248-257).  Outputs in the
+// engine's fixed coefficient layout [a0; a_2..a_10; b_2..b_10].
+template <class T>
+__global__ void k_geometry(DevPtrs<T> d, T* lab, T* labR0, T* R, T* dR, T* ddR, T* rmax) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= d.Ntot) return;
+    const int s = d.sim_of[g];
+    const SimDesc<T>& P = d.sims[s];
+    const T* rc = rec_cur(d, d.clock[s]) + (size_t)g * RECW;
+    const T* cf = d.coef + (size_t)g * NCM;
+    const T r0 = d.R0[g];
+    const T th = rc[R_TH];
+    lab[(size_t)g * NCM] = cf[0];
+    labR0[(size_t)g * NCM] = rc[R_A0];
+    for (int m = 0; m < KM; ++m) {
+        T al = T(0), be = T(0);
+        if (m < P.K) {
+            T so, co;
+            t_sincos(T(m + 2) * th, &so, &co);
+            al = cf[1 + m] * co - cf[1 + KM + m] * so;
+            be = cf[1 + m] * so + cf[1 + KM + m] * co;
+        }
+        lab[(size_t)g * NCM + 1 + m] = al;
+        lab[(size_t)g * NCM + 1 + KM + m] = be;
+        labR0[(size_t)g * NCM + 1 + m] = rc[R_AL + m];
+        labR0[(size_t)g * NCM + 1 + KM + m] = rc[R_BE + m];
+    }
+    rmax[g] = rc[R_RMAX];
+    for (int k = 0; k < P.nth; ++k) {
+        const T c1 = d.cs[2 * k], s1 = d.cs[2 * k + 1];
+        T c = c1, sn = s1, r = rc[R_A0], r1 = T(0), r2 = T(0);
+        for (int m = 0; m < KM; ++m) {
+            const T n = T(m + 2);
+            const T cn = c * c1 - sn * s1;
+            sn = sn * c1 + c * s1;
+            c = cn;
+            const T al = rc[R_AL + m], be = rc[R_BE + m];
+            const T t = al * c + be * sn;
+            r += t;
+            r1 += n * (be * c - al * sn);
+            r2 -= n * n * t;
+        }
+        R[(size_t)g * P.nth + k] = r;
+        dR[(size_t)g * P.nth + k] = r1;
+        ddR[(size_t)g * P.nth + k] = r2;
+    }
+}
+
+// perimeters, areas, shape index with FP64 node sums (src/observables.jl:7-18).
+template <class T>
+__global__ void k_observables(DevPtrs<T> d, double* out) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= d.Ntot) return;
+    const int s = d.sim_of[g];
+    const SimDesc<T>& P = d.sims[s];
+    const T* rc = rec_cur(d, d.clock[s]) + (size_t)g * RECW;
+    double per = 0.0, area = 0.0;
+    for (int k = 0; k < P.nth; ++k) {
+        const T c1 = d.cs[2 * k], s1 = d.cs[2 * k + 1];
+        T c = c1, sn = s1, r = rc[R_A0], r1 = T(0);
+        for (int m = 0; m < KM; ++m) {
+            const T n = T(m + 2);
+            const T cn = c * c1 - sn * s1;
+            sn = sn * c1 + c * s1;
+            c = cn;
+            const T al = rc[R_AL + m], be = rc[R_BE + m];
+            r += al * c + be * sn;
+            r1 += n * (be * c - al * sn);
+        }
+        per += sqrt((double)r * r + (double)r1 * r1);
+        area += (double)r * r;
+    }
+    per *= (double)P.dphi;
+    area *= (double)P.dphi / 2.0;
+    out[3 * (size_t)g] = per;
+    out[3 * (size_t)g + 1] = area;
+    out[3 * (size_t)g + 2] = per / sqrt(area);
+}
+
+// philox_noise! (src/random.jl:113-130): first three normals of body i.
+template <class T>
+__global__ void k_noise(uint32_t k0, uint32_t k1, uint64_t draw, int n, T* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    T z1, z2, z3, z4;
+    philox_pair<T>(k0, k1, (uint32_t)(i + 1), draw, 0u, z1, z2);
+    philox_pair<T>(k0, k1, (uint32_t)(i + 1), draw, 1u, z3, z4);
+    out[3 * (size_t)i] = z1;
+    out[3 * (size_t)i + 1] = z2;
+    out[3 * (size_t)i + 2] = z3;
+}
+
+// Pack caller x, y, rmax into records for the stateless neighbour build.
+template <class T>
+__global__ void k_pack_head(T* rec, const T* x, const T* y, const T* rmax, int n) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    rec[(size_t)g * RECW + R_X] = x[g];
+    rec[(size_t)g * RECW + R_Y] = y[g];
+    rec[(size_t)g * RECW + R_RMAX] = rmax[g];
+}
+
+}  // namespace fcc

@@ -1,0 +1,1149 @@
+// fcc_lib.cu — host runtime of libfcc_b200: the C ABI of include/fcc.h.
+//
+// An Engine<T> owns the device state of one simulation (the body, cell and
+// neighbour arrays of fcc_device.cuh), one CUDA stream and the launch
+// configuration of the persistent step kernel.  Every reference entry point
+// maps onto it: Simulation(...) -> fcc_create (src/simulation.jl:66-105),
+// step! -> fcc_step (:165-173), run! -> fcc_run (:220-235 and
+// ext/FourierContourCellsCUDAExt.jl:144-180), compute_gradients! ->
+// fcc_compute_gradients (:150-158), update_neighbors! -> fcc_update_neighbors
+// (:132-142), shape_index & co. -> fcc_shape_index (src/observables.jl:7-18).
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <set>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/fcc.h"
+#include "fcc_kernels.cuh"
+
+using namespace fcc;
+
+namespace {
+
+thread_local std::string g_err;
+
+fcc_status fail(fcc_status code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+fcc_status cuda_fail(cudaError_t e, const char* what) {
+    g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? FCC_ERR_NOMEM : FCC_ERR_CUDA;
+}
+#define CUDA_TRY(x)                                      \
+    do {                                                 \
+        cudaError_t e_ = (x);                            \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #x); \
+    } while (0)
+#define FCC_TRY(x)                        \
+    do {                                  \
+        fcc_status s_ = (x);              \
+        if (s_ != FCC_OK) return s_;      \
+    } while (0)
+
+// Device buffer owned by an engine.
+template <class V>
+struct DBuf {
+    V* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    fcc_status alloc(size_t count, cudaStream_t st) {
+        release();
+        n = count;
+        if (count == 0) return FCC_OK;
+        CUDA_TRY(cudaMalloc(&p, count * sizeof(V)));
+        CUDA_TRY(cudaMemsetAsync(p, 0, count * sizeof(V), st));
+        return FCC_OK;
+    }
+    fcc_status upload(const std::vector<V>& h, cudaStream_t st) {
+        FCC_TRY(alloc(h.size(), st));
+        if (!h.empty()) CUDA_TRY(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice, st));
+        return FCC_OK;
+    }
+};
+
+const double PI = 3.14159265358979323846;
+
+// Launch configuration of the force/update kernels for nθ (lanes per body,
+// node slots per lane); see fcc_kernels.cuh.
+constexpr int LANES = 8, SLOTS = 5, BLOCK = 256;
+
+struct EngineBase {
+    virtual ~EngineBase() = default;
+    virtual fcc_status step(int64_t n, bool eager) = 0;
+    virtual fcc_status run(fcc_sim* h, int64_t n, int64_t every, fcc_callback cb, void* user, bool graph) = 0;
+    virtual fcc_status update_neighbors(bool force) = 0;
+    virtual fcc_status compute_gradients() = 0;
+    virtual fcc_status get_state(fcc_bodies_host* out, int64_t* clock, double* t, int64_t* stp) = 0;
+    virtual fcc_status set_state(const fcc_bodies_host* in, int64_t clock) = 0;
+    virtual fcc_status set_dt(double dt) = 0;
+    virtual fcc_status get_gradients(const fcc_gradients_host* out) = 0;
+    virtual fcc_status get_geometry(const fcc_geometry_host* out) = 0;
+    virtual fcc_status neighbor_dims(int32_t*, int32_t*, int32_t*, int64_t*, int32_t*) = 0;
+    virtual fcc_status get_neighbors(const fcc_neighbors_host* out) = 0;
+    virtual fcc_status observable(int which, int32_t type, double* out, int64_t* count) = 0;
+    virtual fcc_status body_energy(double* out) = 0;
+    virtual fcc_status timing(double* ms, int64_t* launches, int64_t* steps) = 0;
+};
+
+template <class T>
+struct Engine final : EngineBase {
+    int device = 0, nsm = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // configuration
+    int64_t N = 0;
+    int K = 0, nc = 0, nth = 0, cap = 32, ncx = 1, ncy = 1;
+    bool has_contact = false, split = false;
+    SimDesc<T> desc{};
+    std::vector<int32_t> type_h, parent_h;
+    std::vector<T> R0_h;
+    // host mirror of run state
+    long long clock_h = 0;
+    T t_h = T(0);
+    int64_t step_h = 0;
+    int64_t builds_adjust = 0;
+    double last_ms = 0;
+    int64_t last_launches = 0, last_steps = 0;
+    int step_grid = 0;
+    // device buffers
+    DBuf<SimDesc<T>> sims;
+    DBuf<T> rec0, rec1, coef, R0, x0, y0, rmax0, cs, gx, gy, gth, glab, E, P, GR, GD, GDD, gcoef;
+    DBuf<int> imgx, imgy, sim_of, nb_idx, nb_count, cellid, slot, perm, cstart, cstop, ccount, cell_sim, ch_idx,
+        ch_count, bd_idx, bd_count, flags, maxcount;
+    DBuf<long long> clock, builds;
+    DBuf<GridSync> sync;
+    int ccap = 1, bcap = 1;
+    // pinned read-back of the run state
+    struct Status {
+        int flags, maxcount;
+        long long clock, builds;
+        GridSync sync;
+    };
+    Status* st_h = nullptr;
+
+    ~Engine() override {
+        if (stream) cudaStreamSynchronize(stream);
+        if (st_h) cudaFreeHost(st_h);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    DevPtrs<T> ptrs() const {
+        DevPtrs<T> d{};
+        d.sims = sims.p;
+        d.nsims = 1;
+        d.Ntot = (int)N;
+        d.Ctot = ncx * ncy;
+        d.nth = nth;
+        d.cap = cap;
+        d.sim_of = sim_of.p;
+        d.rec0 = rec0.p;
+        d.rec1 = rec1.p;
+        d.coef = coef.p;
+        d.imgx = imgx.p;
+        d.imgy = imgy.p;
+        d.R0 = R0.p;
+        d.x0 = x0.p;
+        d.y0 = y0.p;
+        d.rmax0 = rmax0.p;
+        d.nb_idx = nb_idx.p;
+        d.nb_count = nb_count.p;
+        d.cellid = cellid.p;
+        d.slot = slot.p;
+        d.perm = perm.p;
+        d.cstart = cstart.p;
+        d.cstop = cstop.p;
+        d.ccount = ccount.p;
+        d.cell_sim = cell_sim.p;
+        d.ccap = ccap;
+        d.ch_idx = ch_idx.p;
+        d.ch_count = ch_count.p;
+        d.bcap = bcap;
+        d.bd_idx = bd_idx.p;
+        d.bd_count = bd_count.p;
+        d.flags = flags.p;
+        d.clock = clock.p;
+        d.builds = builds.p;
+        d.maxcount = maxcount.p;
+        d.sync = sync.p;
+        d.cs = cs.p;
+        d.gx = gx.p;
+        d.gy = gy.p;
+        d.gth = gth.p;
+        d.glab = glab.p;
+        d.E = E.p;
+        d.P = P.p;
+        d.GR = GR.p;
+        d.GD = GD.p;
+        d.GDD = GDD.p;
+        d.gcoef = gcoef.p;
+        return d;
+    }
+
+    // ------------------------------------------------------------ set-up --
+    fcc_status init(const fcc_params* p, const fcc_bodies_host* b) {
+        // validation in the order of src/simulation.jl:66-105
+        if (!p || !b) return fail(FCC_ERR_ARGUMENT, "null argument");
+        if (p->ntypes < 1 || p->ntypes > FCC_MAX_TYPES || !p->types)
+            return fail(FCC_ERR_ARGUMENT, "types must hold 1..8 BodyType entries");
+        for (int t = 0; t < p->ntypes; ++t)
+            if (p->types[t].parent_drag != 0 && p->types[t].parent_drag != 1)
+                return fail(FCC_ERR_ARGUMENT, "drag must be :substrate or :parent");
+        if (p->nterms < 0 || p->nterms > FCC_MAX_TERMS || (p->nterms > 0 && !p->terms))
+            return fail(FCC_ERR_ARGUMENT, "energy terms must be BodyTerms, ContactTerms or BondTerms");
+        for (int q = 0; q < p->nterms; ++q) {
+            const fcc_term& ft = p->terms[q];
+            if (ft.kind < FCC_TENSION || ft.kind > FCC_HARMONIC_BOND)
+                return fail(FCC_ERR_ARGUMENT, "energy terms must be BodyTerms, ContactTerms or BondTerms");
+            if (ft.ntypes_on < 0 || ft.ntypes_on > FCC_MAX_TYPES) return fail(FCC_ERR_ARGUMENT, "OnTypes: bad type list");
+            if (ft.kind == FCC_OVERLAP && (ft.nJ < 1 || ft.nJ > FCC_MAX_TYPES))
+                return fail(FCC_ERR_DIMENSION, "coupling tables must be square and equal-sized");
+        }
+        N = b->n;
+        if (N < 0) return fail(FCC_ERR_DIMENSION, "inconsistent body array lengths");
+        if (N > (1 << 27)) return fail(FCC_ERR_UNSUPPORTED, "at most 2^27 bodies per simulation");
+        int32_t maxtype = 0;
+        for (int64_t i = 0; i < N; ++i) {
+            if (b->type[i] > p->ntypes) return fail(FCC_ERR_ARGUMENT, "body type without BodyType entry");
+            if (b->type[i] < 1) return fail(FCC_ERR_ARGUMENT, "body type ids are 1-based");
+            maxtype = std::max(maxtype, b->type[i]);
+        }
+        for (int q = 0; q < p->nterms; ++q) {
+            const fcc_term& ft = p->terms[q];
+            if (ft.kind == FCC_OVERLAP && ft.nJ > 1 && ft.nJ < maxtype)
+                return fail(FCC_ERR_DIMENSION, "Overlap coupling table smaller than the number of body types");
+        }
+        for (int64_t i = 0; i < N; ++i) {  // check_parents, src/simulation.jl:108-118
+            int64_t pp = b->parent[i];
+            if (pp < 1 || pp > N)
+                return fail(FCC_ERR_ARGUMENT, "body " + std::to_string(i + 1) + " has parent " + std::to_string(pp) +
+                                                  " outside 1:" + std::to_string(N));
+            if (!p->types[b->type[i] - 1].parent_drag) continue;
+            if (pp == i + 1)
+                return fail(FCC_ERR_ARGUMENT, "body " + std::to_string(i + 1) + " has drag = :parent but is its own parent");
+            if (p->types[b->type[pp - 1] - 1].parent_drag)
+                return fail(FCC_ERR_ARGUMENT, "body " + std::to_string(i + 1) + " has drag = :parent, but so has its parent " +
+                                                  std::to_string(pp) + " (one level only)");
+        }
+        K = b->ncoef / 2;
+        nth = p->ntheta;
+        if (K + 1 < 2) return fail(FCC_ERR_ARGUMENT, "maxmode must be ≥ 2");
+        if (!(nth > 2 * (K + 1))) return fail(FCC_ERR_ARGUMENT, "nθ must exceed 2·maxmode");
+        nc = 2 * K + 1;
+        if (b->ncoef != nc) return fail(FCC_ERR_DIMENSION, "coefficient rows must be odd: [a₀; aₙ; bₙ]");
+        if (K > KM) return fail(FCC_ERR_UNSUPPORTED, "this build supports maxmode ≤ 10");
+        if (!(p->skin >= 0)) return fail(FCC_ERR_ARGUMENT, "skin must be non-negative");
+
+        // device and stream
+        CUDA_TRY(cudaGetDevice(&device));
+        CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+        int coop = 0;
+        CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+        if (!coop) return fail(FCC_ERR_UNSUPPORTED, "device lacks cooperative launch");
+        CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreate(&ev0));
+        CUDA_TRY(cudaEventCreate(&ev1));
+        CUDA_TRY(cudaMallocHost(&st_h, sizeof(Status)));
+
+        // simulation descriptor (convert_precision: every parameter to T)
+        SimDesc<T>& s = desc;
+        s.Lx = (T)p->Lx;
+        s.Ly = (T)p->Ly;
+        s.invLx = T(1) / s.Lx;
+        s.invLy = T(1) / s.Ly;
+        s.dt = (T)p->dt;
+        s.skin = (T)p->skin;
+        s.crange = T(0);  // interaction_range of the built-in contact terms
+        s.nbrange = s.crange + s.skin;
+        s.dphi = (T)(2 * PI / nth);
+        R0_h.resize(N);
+        double maxR0 = 0;
+        for (int64_t i = 0; i < N; ++i) {
+            R0_h[i] = (T)b->R0[i];
+            maxR0 = std::max(maxR0, (double)R0_h[i]);
+        }
+        const double cutoff = 2 * maxR0 * (1 + SHAPE_BOUND) + 0.0 + p->skin;  // src/simulation.jl:90
+        auto ncells = [&](T L) {
+            int64_t n = (int64_t)std::floor((double)L / cutoff);
+            return (int)(n >= 3 ? n : 1);
+        };
+        ncx = ncells(s.Lx);
+        ncy = ncells(s.Ly);
+        if ((int64_t)ncx * ncy > (1 << 28)) return fail(FCC_ERR_UNSUPPORTED, "cell grid too large");
+        s.wx = s.Lx / (T)ncx;
+        s.wy = s.Ly / (T)ncy;
+        s.ncx = ncx;
+        s.ncy = ncy;
+        s.cell_off = 0;
+        s.ncells = ncx * ncy;
+        s.body_off = 0;
+        s.n = (int)N;
+        s.nth = nth;
+        s.K = K;
+        s.k0 = (uint32_t)(p->seed & 0xffffffffu);
+        s.k1 = (uint32_t)(p->seed >> 32);
+        s.ntypes = p->ntypes;
+        s.rewrap = (ncx < 3 || ncy < 3) ? 1 : 0;
+        for (int t = 0; t < p->ntypes; ++t) {
+            const fcc_body_type& bt = p->types[t];
+            s.v0[t] = (T)bt.v0;
+            s.Dr[t] = (T)bt.Dr;
+            s.Dt[t] = (T)bt.Dt;
+            s.mur[t] = (T)bt.mu_r;
+            s.muth[t] = (T)bt.mu_theta;
+            s.muab[t] = (T)bt.mu_ab;
+            s.parent_drag[t] = bt.parent_drag;
+        }
+        auto mask_of = [](const fcc_term& ft) {
+            if (ft.ntypes_on == 0) return 0xffffffffu;
+            uint32_t m = 0;
+            for (int u = 0; u < ft.ntypes_on; ++u)
+                if (ft.types_on[u] >= 1 && ft.types_on[u] <= FCC_MAX_TYPES) m |= 1u << (ft.types_on[u] - 1);
+            return m;
+        };
+        // contact couplings summed over terms in the reference's order g1 + (g2 + ...)
+        for (int r = 0; r < 2; ++r)
+            for (int a = 0; a < MT; ++a)
+                for (int c = 0; c < MT; ++c) s.cA[r][a][c] = T(0);
+        for (int a = 0; a < MT; ++a) s.cB[a] = T(0);
+        for (int q = p->nterms - 1; q >= 0; --q) {
+            const fcc_term& ft = p->terms[q];
+            const uint32_t mk = mask_of(ft);
+            if (ft.kind == FCC_OVERLAP) {
+                has_contact = true;
+                for (int a = 0; a < MT; ++a) {
+                    if (!((mk >> a) & 1u)) continue;
+                    for (int c = 0; c < MT; ++c) {
+                        const int ij = ft.nJ == 1 ? 0 : (a < ft.nJ && c < ft.nJ ? a + ft.nJ * c : -1);
+                        if (ij < 0) continue;
+                        s.cA[0][a][c] = (T)ft.J[ij] + s.cA[0][a][c];
+                        s.cA[1][a][c] = (T)ft.Jrel[ij] + s.cA[1][a][c];
+                    }
+                }
+            } else if (ft.kind == FCC_LINEAR_REPULSION) {
+                has_contact = true;
+                for (int a = 0; a < MT; ++a)
+                    if ((mk >> a) & 1u) s.cB[a] = (T)ft.a + s.cB[a];
+            }
+        }
+        s.nbt = 0;
+        s.nbd = 0;
+        for (int q = 0; q < p->nterms; ++q) {
+            const fcc_term& ft = p->terms[q];
+            if (ft.kind == FCC_TENSION || ft.kind == FCC_PERIMETER_ELASTICITY) {
+                const int u = s.nbt++;
+                s.bt_kind[u] = ft.kind == FCC_TENSION ? BT_TENSION : BT_PERIMETER;
+                s.bt_mask[u] = mask_of(ft);
+                s.bt_a[u] = (T)ft.a;
+                // l0 = p0 * sqrt(π) * R0 (src/energies/body_terms.jl:34)
+                s.bt_b[u] = ft.kind == FCC_TENSION ? T(0) : (T)ft.b * std::sqrt((T)PI);
+            } else if (ft.kind == FCC_HARMONIC_BOND) {
+                const int u = s.nbd++;
+                s.bd_mask[u] = mask_of(ft);
+                s.bd_k[u] = (T)ft.a;
+                s.bd_r0[u] = (T)ft.b;
+            }
+        }
+        s.has_contact = has_contact ? 1 : 0;
+        split = false;
+        for (int64_t i = 0; i < N; ++i)
+            if (p->types[b->type[i] - 1].parent_drag) split = true;
+        s.has_parent_drag = split ? 1 : 0;
+
+        // children (src/bodies.jl:121-135) and bonds (src/energies/bonds.jl:52-71), global ids
+        type_h.assign(b->type, b->type + N);
+        parent_h.assign(b->parent, b->parent + N);
+        std::vector<int> chc(N, 0);
+        for (int64_t k = 0; k < N; ++k)
+            if (parent_h[k] != k + 1) chc[parent_h[k] - 1] += 1;
+        ccap = 1;
+        for (int64_t k = 0; k < N; ++k) ccap = std::max(ccap, chc[k]);
+        std::vector<int> chi((size_t)ccap * N, 0);
+        std::fill(chc.begin(), chc.end(), 0);
+        for (int64_t k = 0; k < N; ++k) {
+            const int pp = parent_h[k] - 1;
+            if (pp == k) continue;
+            chi[(size_t)pp * ccap + chc[pp]++] = (int)k;
+        }
+        std::vector<int> bdc(N, 0);
+        std::set<std::pair<int64_t, int64_t>> seen;
+        for (int64_t q = 0; q < p->nbonds; ++q) {
+            const int64_t i = p->bonds[2 * q], j = p->bonds[2 * q + 1];
+            if (!(1 <= i && i <= N && 1 <= j && j <= N))
+                return fail(FCC_ERR_ARGUMENT, "bond (" + std::to_string(i) + ", " + std::to_string(j) +
+                                                  ") refers to a body outside 1:" + std::to_string(N));
+            if (i == j)
+                return fail(FCC_ERR_ARGUMENT, "bond (" + std::to_string(i) + ", " + std::to_string(j) + ") connects a body to itself");
+            auto key = std::make_pair(std::min(i, j), std::max(i, j));
+            if (seen.count(key)) return fail(FCC_ERR_ARGUMENT, "duplicate bond (" + std::to_string(i) + ", " + std::to_string(j) + ")");
+            seen.insert(key);
+            bdc[i - 1] += 1;
+            bdc[j - 1] += 1;
+        }
+        bcap = 1;
+        for (int64_t k = 0; k < N; ++k) bcap = std::max(bcap, bdc[k]);
+        std::vector<int> bdi((size_t)bcap * N, 0);
+        std::fill(bdc.begin(), bdc.end(), 0);
+        for (int64_t q = 0; q < p->nbonds; ++q) {
+            const int64_t i = p->bonds[2 * q] - 1, j = p->bonds[2 * q + 1] - 1;
+            bdi[(size_t)i * bcap + bdc[i]++] = (int)j;
+            bdi[(size_t)j * bcap + bdc[j]++] = (int)i;
+        }
+
+        // device buffers
+        cap = p->nl_capacity > 0 ? p->nl_capacity : 32;
+        const size_t n = (size_t)N;
+        FCC_TRY(sims.upload(std::vector<SimDesc<T>>{desc}, stream));
+        FCC_TRY(rec0.alloc(n * RECW, stream));
+        FCC_TRY(rec1.alloc(n * RECW, stream));
+        FCC_TRY(coef.alloc(n * NCM, stream));
+        FCC_TRY(R0.upload(R0_h, stream));
+        FCC_TRY(x0.alloc(n, stream));
+        FCC_TRY(y0.alloc(n, stream));
+        FCC_TRY(rmax0.alloc(n, stream));
+        FCC_TRY(gx.alloc(n, stream));
+        FCC_TRY(gy.alloc(n, stream));
+        FCC_TRY(gth.alloc(n, stream));
+        FCC_TRY(E.alloc(n, stream));
+        FCC_TRY(glab.alloc(n * NCM, stream));
+        std::vector<T> csh(2 * (size_t)nth);
+        for (int k = 0; k < nth; ++k) {  // FourierBasis.cs, src/basis.jl:50-52
+            const double phi = k * (2 * PI / nth);
+            csh[2 * k] = (T)std::cos(phi);
+            csh[2 * k + 1] = (T)std::sin(phi);
+        }
+        FCC_TRY(cs.upload(csh, stream));
+        FCC_TRY(imgx.upload(std::vector<int>(b->imgx, b->imgx + N), stream));
+        FCC_TRY(imgy.upload(std::vector<int>(b->imgy, b->imgy + N), stream));
+        FCC_TRY(sim_of.alloc(n, stream));
+        FCC_TRY(nb_idx.alloc(n * cap, stream));
+        FCC_TRY(nb_count.alloc(n, stream));
+        FCC_TRY(cellid.alloc(n, stream));
+        FCC_TRY(slot.alloc(n, stream));
+        FCC_TRY(perm.alloc(n, stream));
+        FCC_TRY(cstart.alloc((size_t)ncx * ncy, stream));
+        FCC_TRY(cstop.alloc((size_t)ncx * ncy, stream));
+        FCC_TRY(ccount.alloc((size_t)ncx * ncy, stream));
+        FCC_TRY(cell_sim.alloc((size_t)ncx * ncy, stream));
+        FCC_TRY(ch_idx.upload(chi, stream));
+        FCC_TRY(ch_count.upload(chc, stream));
+        FCC_TRY(bd_idx.upload(bdi, stream));
+        FCC_TRY(bd_count.upload(bdc, stream));
+        FCC_TRY(flags.upload(std::vector<int>{F_ACTIVE | (has_contact ? F_CONTACT : 0)}, stream));
+        FCC_TRY(maxcount.alloc(1, stream));
+        FCC_TRY(clock.alloc(1, stream));
+        FCC_TRY(builds.alloc(1, stream));
+        FCC_TRY(sync.alloc(1, stream));
+
+        // launch configuration of the persistent kernel: all co-resident blocks
+        FCC_TRY(configure());
+        FCC_TRY(load_state(b, 0));
+        return sync_stream();
+    }
+
+    template <class F>
+    fcc_status occupancy(F kernel, int& blocks) {
+        int per_sm = 0;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, BLOCK, 0));
+        if (per_sm < 1) return fail(FCC_ERR_UNSUPPORTED, "step kernel does not fit on an SM");
+        blocks = per_sm * nsm;
+        return FCC_OK;
+    }
+
+    bool one_chunk() const { return nth <= LANES * SLOTS; }
+
+    fcc_status configure() {
+        int maxblocks = 0;
+        if (one_chunk())
+            FCC_TRY(split ? occupancy(k_step<T, LANES, SLOTS, true, true>, maxblocks)
+                          : occupancy(k_step<T, LANES, SLOTS, true, false>, maxblocks));
+        else
+            FCC_TRY(split ? occupancy(k_step<T, LANES, SLOTS, false, true>, maxblocks)
+                          : occupancy(k_step<T, LANES, SLOTS, false, false>, maxblocks));
+        const int64_t groups = (N + (32 / LANES) - 1) / (32 / LANES);
+        const int64_t want = std::max<int64_t>(1, (groups + BLOCK / 32 - 1) / (BLOCK / 32));
+        step_grid = (int)std::min<int64_t>(want, maxblocks);
+        return FCC_OK;
+    }
+
+    // Copy a host body state in and rebuild the derived geometry (k_init).
+    fcc_status load_state(const fcc_bodies_host* b, int64_t clk) {
+        const size_t n = (size_t)N;
+        std::vector<T> hx(n), hy(n), hth(n), hc(n * NCM, T(0));
+        std::vector<int> w(n), so(n, 0), cellsim((size_t)ncx * ncy, 0);
+        for (size_t i = 0; i < n; ++i) {
+            hx[i] = (T)b->x[i];
+            hy[i] = (T)b->y[i];
+            hth[i] = (T)b->theta[i];
+            const double* c = b->coef + i * nc;
+            hc[i * NCM] = (T)c[0];
+            for (int m = 0; m < K; ++m) {
+                hc[i * NCM + 1 + m] = (T)c[1 + m];
+                hc[i * NCM + 1 + KM + m] = (T)c[1 + K + m];
+            }
+            w[i] = ((parent_h[i] - 1) << 3) | (type_h[i] - 1);
+        }
+        if (clk >= 0) clock_h = clk;
+        DBuf<T> bx, by, bth, bc;
+        DBuf<int> bw;
+        FCC_TRY(bx.upload(hx, stream));
+        FCC_TRY(by.upload(hy, stream));
+        FCC_TRY(bth.upload(hth, stream));
+        FCC_TRY(bc.upload(hc, stream));
+        FCC_TRY(bw.upload(w, stream));
+        CUDA_TRY(cudaMemcpyAsync(clock.p, &clock_h, sizeof(long long), cudaMemcpyHostToDevice, stream));
+        if (b->imgx) CUDA_TRY(cudaMemcpyAsync(imgx.p, b->imgx, n * sizeof(int), cudaMemcpyHostToDevice, stream));
+        if (b->imgy) CUDA_TRY(cudaMemcpyAsync(imgy.p, b->imgy, n * sizeof(int), cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(cudaMemcpyAsync(sim_of.p, so.data(), n * sizeof(int), cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(cudaMemcpyAsync(cell_sim.p, cellsim.data(), cellsim.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+        const DevPtrs<T> d = ptrs();
+        if (N > 0) {
+            const int grid = (int)((N + 255) / 256);
+            k_init<T><<<grid, 256, 0, stream>>>(d, bx.p, by.p, bth.p, bc.p);
+            CUDA_TRY(cudaGetLastError());
+            k_set_w<T><<<grid, 256, 0, stream>>>(d, bw.p);
+            CUDA_TRY(cudaGetLastError());
+        }
+        // list invalid: the next step (or update_neighbors!) rebuilds
+        const int f = F_ACTIVE | (has_contact ? (F_CONTACT | F_NEED) : 0);
+        CUDA_TRY(cudaMemcpyAsync(flags.p, &f, sizeof(int), cudaMemcpyHostToDevice, stream));
+        GridSync gs{0, 0, 0, has_contact ? 1 : 0};
+        CUDA_TRY(cudaMemcpyAsync(sync.p, &gs, sizeof(GridSync), cudaMemcpyHostToDevice, stream));
+        return sync_stream();  // staging buffers are freed on return
+    }
+
+    fcc_status sync_stream() {
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        return FCC_OK;
+    }
+
+    fcc_status read_status() {
+        CUDA_TRY(cudaMemcpyAsync(&st_h->flags, flags.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaMemcpyAsync(&st_h->maxcount, maxcount.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaMemcpyAsync(&st_h->clock, clock.p, sizeof(long long), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaMemcpyAsync(&st_h->builds, builds.p, sizeof(long long), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaMemcpyAsync(&st_h->sync, sync.p, sizeof(GridSync), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        if (st_h->sync.error) return fail(FCC_ERR_DEVICE, "a grid barrier wait timed out in the step kernel");
+        return FCC_OK;
+    }
+
+    // Account executed steps (t accumulates in T, as sim.t += sim.dt does).
+    void account(long long newclock) {
+        const long long executed = newclock - clock_h;
+        for (long long q = 0; q < executed; ++q) t_h += desc.dt;
+        step_h += executed;
+        clock_h = newclock;
+    }
+
+    // Neighbour-list overflow: grow the capacity to twice the largest count
+    // (src/neighbors.jl:226-233) and rebuild at the next step.
+    fcc_status regrow() {
+        const int newcap = std::max(2 * st_h->maxcount, cap + 1);
+        FCC_TRY(nb_idx.alloc((size_t)N * newcap, stream));
+        cap = newcap;
+        builds_adjust -= 1;  // the overflowed build is repeated
+        const int f = (st_h->flags & ~(F_FROZEN | F_VALID | F_REBUILD)) | F_NEED;
+        CUDA_TRY(cudaMemcpyAsync(flags.p, &f, sizeof(int), cudaMemcpyHostToDevice, stream));
+        const int one = 1;
+        CUDA_TRY(cudaMemcpyAsync(&sync.p->any_need, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
+        return sync_stream();
+    }
+
+    fcc_status launch_steps(int nsteps) {
+        DevPtrs<T> d = ptrs();
+        void* args[] = {&d, &nsteps};
+        void* fn;
+        if (one_chunk())
+            fn = split ? (void*)k_step<T, LANES, SLOTS, true, true> : (void*)k_step<T, LANES, SLOTS, true, false>;
+        else
+            fn = split ? (void*)k_step<T, LANES, SLOTS, false, true> : (void*)k_step<T, LANES, SLOTS, false, false>;
+        CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(step_grid), dim3(BLOCK), args, 0, stream));
+        ++last_launches;
+        return FCC_OK;
+    }
+
+    // Run n steps as launches of `per` steps each.  A neighbour-list overflow
+    // freezes the simulation on the device (the remaining launched steps do
+    // nothing); the host then regrows the list and launches the missing steps.
+    fcc_status advance(int64_t n, int per) {
+        int64_t done = 0;
+        while (done < n) {
+            const long long start = clock_h;
+            const int64_t requested = n - done;
+            for (int64_t remaining = requested; remaining > 0;) {
+                const int k = (int)std::min<int64_t>(per, remaining);
+                FCC_TRY(launch_steps(k));
+                remaining -= k;
+            }
+            FCC_TRY(read_status());
+            account(st_h->clock);
+            const int64_t executed = st_h->clock - start;
+            done += executed;
+            if (st_h->flags & F_FROZEN) FCC_TRY(regrow());
+            else if (executed < requested) return fail(FCC_ERR_DEVICE, "step kernel did not advance the clock");
+        }
+        return FCC_OK;
+    }
+
+    fcc_status step(int64_t n, bool eager) override {
+        if (n <= 0 || N == 0) {
+            if (n > 0) {  // no bodies: only the clock and time advance
+                for (int64_t q = 0; q < n; ++q) t_h += desc.dt;
+                step_h += n;
+                clock_h += n;
+                CUDA_TRY(cudaMemcpyAsync(clock.p, &clock_h, sizeof(long long), cudaMemcpyHostToDevice, stream));
+                return sync_stream();
+            }
+            return FCC_OK;
+        }
+        last_launches = 0;
+        const long long c0 = clock_h;
+        CUDA_TRY(cudaEventRecord(ev0, stream));
+        FCC_TRY(advance(n, eager ? 1 : 512));
+        CUDA_TRY(cudaEventRecord(ev1, stream));
+        CUDA_TRY(cudaEventSynchronize(ev1));
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
+        last_ms = ms;
+        last_steps = clock_h - c0;
+        return FCC_OK;
+    }
+
+    fcc_status run(fcc_sim* h, int64_t n, int64_t every, fcc_callback cb, void* user, bool graph) override {
+        if (!cb || every <= 0) return step(n, !graph);
+        int64_t done = 0;
+        while (done < n) {
+            const int64_t k = std::min(every, n - done);
+            FCC_TRY(step(k, !graph));
+            done += k;
+            cb(h, user);
+        }
+        return FCC_OK;
+    }
+
+    fcc_status update_neighbors(bool force) override {
+        if (!has_contact || N == 0) return FCC_OK;
+        const DevPtrs<T> d = ptrs();
+        const int grid = (int)((N + 255) / 256);
+        for (int attempt = 0; attempt < 8; ++attempt) {
+            DevPtrs<T> dd = ptrs();
+            if (!force && attempt == 0) {
+                k_skin_check<T><<<grid, 256, 0, stream>>>(dd);
+                CUDA_TRY(cudaGetLastError());
+            }
+            k_prepare_rebuild<T><<<1, 256, 0, stream>>>(dd, (force || attempt > 0) ? 1 : 0);
+            k_phase_count<T><<<grid, 256, 0, stream>>>(dd);
+            k_phase_scan<T><<<1, 1024, 0, stream>>>(dd);
+            k_phase_scatter<T><<<grid, 256, 0, stream>>>(dd);
+            k_phase_sort<T><<<(ncx * ncy + 255) / 256, 256, 0, stream>>>(dd);
+            k_phase_neighbors<T><<<grid, 256, 0, stream>>>(dd);
+            k_finish_rebuild<T><<<1, 256, 0, stream>>>(dd);
+            CUDA_TRY(cudaGetLastError());
+            FCC_TRY(read_status());
+            if (!(st_h->flags & F_FROZEN)) return FCC_OK;
+            FCC_TRY(regrow());
+        }
+        (void)d;
+        return fail(FCC_ERR_DEVICE, "neighbour list did not fit after regrowth");
+    }
+
+    fcc_status ensure_diag() {
+        if (P.p) return FCC_OK;
+        const size_t n = (size_t)N * nth;
+        FCC_TRY(P.alloc(n, stream));
+        FCC_TRY(GR.alloc(n, stream));
+        FCC_TRY(GD.alloc(n, stream));
+        FCC_TRY(GDD.alloc(n, stream));
+        FCC_TRY(gcoef.alloc((size_t)N * NCM, stream));
+        return FCC_OK;
+    }
+
+    fcc_status compute_gradients() override {
+        if (N == 0) return FCC_OK;
+        FCC_TRY(ensure_diag());
+        const DevPtrs<T> d = ptrs();
+        const int64_t groups = (N + (32 / LANES) - 1) / (32 / LANES);
+        const int grid = (int)((groups + BLOCK / 32 - 1) / (BLOCK / 32));
+        if (one_chunk())
+            k_gradients<T, LANES, SLOTS, true><<<grid, BLOCK, 0, stream>>>(d);
+        else
+            k_gradients<T, LANES, SLOTS, false><<<grid, BLOCK, 0, stream>>>(d);
+        CUDA_TRY(cudaGetLastError());
+        return sync_stream();
+    }
+
+    // engine coefficient layout [a0; a_2..a_10; b_2..b_10] -> reference rows [a0; a_2..a_M; b_2..b_M]
+    void coef_out(const std::vector<T>& src, double* dst) const {
+        for (int64_t i = 0; i < N; ++i) {
+            dst[(size_t)i * nc] = (double)src[(size_t)i * NCM];
+            for (int m = 0; m < K; ++m) {
+                dst[(size_t)i * nc + 1 + m] = (double)src[(size_t)i * NCM + 1 + m];
+                dst[(size_t)i * nc + 1 + K + m] = (double)src[(size_t)i * NCM + 1 + KM + m];
+            }
+        }
+    }
+
+    template <class V>
+    fcc_status fetch(const V* src, size_t n, std::vector<V>& out) {
+        out.resize(n);
+        if (n) CUDA_TRY(cudaMemcpyAsync(out.data(), src, n * sizeof(V), cudaMemcpyDeviceToHost, stream));
+        return FCC_OK;
+    }
+
+    fcc_status get_state(fcc_bodies_host* o, int64_t* clk, double* t, int64_t* stp) override {
+        if (o) {
+            if (o->n != N || o->ncoef != nc) return fail(FCC_ERR_DIMENSION, "state buffers do not match the simulation");
+            std::vector<T> rec, cf;
+            std::vector<int> ix, iy;
+            FCC_TRY(fetch((clock_h & 1) ? rec1.p : rec0.p, (size_t)N * RECW, rec));
+            FCC_TRY(fetch(coef.p, (size_t)N * NCM, cf));
+            FCC_TRY(fetch(imgx.p, (size_t)N, ix));
+            FCC_TRY(fetch(imgy.p, (size_t)N, iy));
+            FCC_TRY(sync_stream());
+            for (int64_t i = 0; i < N; ++i) {
+                if (o->x) o->x[i] = (double)rec[(size_t)i * RECW + R_X];
+                if (o->y) o->y[i] = (double)rec[(size_t)i * RECW + R_Y];
+                if (o->theta) o->theta[i] = (double)rec[(size_t)i * RECW + R_TH];
+                if (o->imgx) o->imgx[i] = ix[i];
+                if (o->imgy) o->imgy[i] = iy[i];
+                if (o->R0) o->R0[i] = (double)R0_h[i];
+                if (o->type) o->type[i] = type_h[i];
+                if (o->parent) o->parent[i] = parent_h[i];
+            }
+            if (o->coef) coef_out(cf, o->coef);
+        }
+        if (clk) *clk = clock_h;
+        if (t) *t = (double)t_h;
+        if (stp) *stp = step_h;
+        return FCC_OK;
+    }
+
+    fcc_status set_state(const fcc_bodies_host* in, int64_t clk) override {
+        if (!in || in->n != N || in->ncoef != nc) return fail(FCC_ERR_DIMENSION, "state buffers do not match the simulation");
+        if (!in->x || !in->y || !in->theta || !in->coef) return fail(FCC_ERR_ARGUMENT, "set_state needs x, y, theta and coef");
+        return load_state(in, clk);
+    }
+
+    fcc_status set_dt(double dt) override {
+        desc.dt = (T)dt;
+        CUDA_TRY(cudaMemcpyAsync(&sims.p->dt, &desc.dt, sizeof(T), cudaMemcpyHostToDevice, stream));
+        return sync_stream();
+    }
+
+    fcc_status get_gradients(const fcc_gradients_host* o) override {
+        if (!o) return fail(FCC_ERR_ARGUMENT, "null argument");
+        if (!P.p) FCC_TRY(ensure_diag());
+        const size_t n = (size_t)N;
+        std::vector<T> a;
+        auto copy_nodes = [&](DBuf<T>& src, double* dst) -> fcc_status {
+            if (!dst) return FCC_OK;
+            FCC_TRY(fetch(src.p, n * nth, a));
+            FCC_TRY(sync_stream());
+            for (size_t q = 0; q < n * nth; ++q) dst[q] = (double)a[q];
+            return FCC_OK;
+        };
+        auto copy_vec = [&](DBuf<T>& src, double* dst) -> fcc_status {
+            if (!dst) return FCC_OK;
+            FCC_TRY(fetch(src.p, n, a));
+            FCC_TRY(sync_stream());
+            for (size_t q = 0; q < n; ++q) dst[q] = (double)a[q];
+            return FCC_OK;
+        };
+        auto copy_coef = [&](DBuf<T>& src, double* dst) -> fcc_status {
+            if (!dst) return FCC_OK;
+            FCC_TRY(fetch(src.p, n * NCM, a));
+            FCC_TRY(sync_stream());
+            coef_out(a, dst);
+            return FCC_OK;
+        };
+        FCC_TRY(copy_nodes(GR, o->GR));
+        FCC_TRY(copy_nodes(GD, o->GD));
+        FCC_TRY(copy_nodes(GDD, o->GDD));
+        FCC_TRY(copy_nodes(P, o->P));
+        FCC_TRY(copy_vec(gx, o->gx));
+        FCC_TRY(copy_vec(gy, o->gy));
+        FCC_TRY(copy_vec(gth, o->gtheta));
+        FCC_TRY(copy_coef(glab, o->glab));
+        FCC_TRY(copy_coef(gcoef, o->gcoef));
+        FCC_TRY(copy_vec(E, o->Ebody));
+        return FCC_OK;
+    }
+
+    fcc_status get_geometry(const fcc_geometry_host* o) override {
+        if (!o) return fail(FCC_ERR_ARGUMENT, "null argument");
+        if (N == 0) return FCC_OK;
+        const size_t n = (size_t)N;
+        DBuf<T> lab, labR0, R, dR, ddR, rmax;
+        FCC_TRY(lab.alloc(n * NCM, stream));
+        FCC_TRY(labR0.alloc(n * NCM, stream));
+        FCC_TRY(R.alloc(n * nth, stream));
+        FCC_TRY(dR.alloc(n * nth, stream));
+        FCC_TRY(ddR.alloc(n * nth, stream));
+        FCC_TRY(rmax.alloc(n, stream));
+        k_geometry<T><<<(int)((N + 127) / 128), 128, 0, stream>>>(ptrs(), lab.p, labR0.p, R.p, dR.p, ddR.p, rmax.p);
+        CUDA_TRY(cudaGetLastError());
+        std::vector<T> a;
+        auto nodes = [&](DBuf<T>& src, double* dst) -> fcc_status {
+            if (!dst) return FCC_OK;
+            FCC_TRY(fetch(src.p, n * nth, a));
+            FCC_TRY(sync_stream());
+            for (size_t q = 0; q < n * nth; ++q) dst[q] = (double)a[q];
+            return FCC_OK;
+        };
+        auto coefs = [&](DBuf<T>& src, double* dst) -> fcc_status {
+            if (!dst) return FCC_OK;
+            FCC_TRY(fetch(src.p, n * NCM, a));
+            FCC_TRY(sync_stream());
+            coef_out(a, dst);
+            return FCC_OK;
+        };
+        FCC_TRY(coefs(lab, o->lab));
+        FCC_TRY(coefs(labR0, o->labR0));
+        FCC_TRY(nodes(R, o->R));
+        FCC_TRY(nodes(dR, o->dR));
+        FCC_TRY(nodes(ddR, o->ddR));
+        if (o->rmax) {
+            FCC_TRY(fetch(rmax.p, n, a));
+            FCC_TRY(sync_stream());
+            for (size_t q = 0; q < n; ++q) o->rmax[q] = (double)a[q];
+        }
+        return sync_stream();
+    }
+
+    fcc_status neighbor_dims(int32_t* cx, int32_t* cy, int32_t* cp, int64_t* b, int32_t* v) override {
+        FCC_TRY(read_status());
+        if (cx) *cx = ncx;
+        if (cy) *cy = ncy;
+        if (cp) *cp = cap;
+        if (b) *b = st_h->builds + builds_adjust;
+        if (v) *v = (st_h->flags & F_VALID) ? 1 : 0;
+        return FCC_OK;
+    }
+
+    fcc_status get_neighbors(const fcc_neighbors_host* o) override {
+        if (!o) return fail(FCC_ERR_ARGUMENT, "null argument");
+        const size_t n = (size_t)N, nce = (size_t)ncx * ncy;
+        std::vector<int> a, b2;
+        if (o->cellid) {
+            FCC_TRY(fetch(cellid.p, n, a));
+            FCC_TRY(sync_stream());
+            for (size_t i = 0; i < n; ++i) o->cellid[i] = a[i] + 1;
+        }
+        if (o->perm) {
+            FCC_TRY(fetch(perm.p, n, a));
+            FCC_TRY(sync_stream());
+            for (size_t i = 0; i < n; ++i) o->perm[i] = a[i] + 1;
+        }
+        if (o->start || o->stop) {
+            FCC_TRY(fetch(cstart.p, nce, a));
+            FCC_TRY(fetch(cstop.p, nce, b2));
+            FCC_TRY(sync_stream());
+            for (size_t c = 0; c < nce; ++c) {
+                const bool empty = b2[c] <= a[c];
+                if (o->start) o->start[c] = empty ? 1 : a[c] + 1;
+                if (o->stop) o->stop[c] = empty ? 0 : b2[c];
+            }
+        }
+        std::vector<int> cnt;
+        FCC_TRY(fetch(nb_count.p, n, cnt));
+        FCC_TRY(sync_stream());
+        if (o->count) std::copy(cnt.begin(), cnt.end(), o->count);
+        if (o->idx) {
+            FCC_TRY(fetch(nb_idx.p, n * cap, a));
+            FCC_TRY(sync_stream());
+            for (size_t i = 0; i < n; ++i)
+                for (int q = 0; q < cap; ++q) o->idx[i * cap + q] = q < cnt[i] ? a[i * cap + q] + 1 : 0;
+        }
+        return FCC_OK;
+    }
+
+    fcc_status observable(int which, int32_t typ, double* out, int64_t* count) override {
+        std::vector<double> v(3 * (size_t)N);
+        if (N > 0) {
+            DBuf<double> buf;
+            FCC_TRY(buf.alloc(3 * (size_t)N, stream));
+            k_observables<T><<<(int)((N + 127) / 128), 128, 0, stream>>>(ptrs(), buf.p);
+            CUDA_TRY(cudaGetLastError());
+            CUDA_TRY(cudaMemcpyAsync(v.data(), buf.p, v.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            FCC_TRY(sync_stream());
+        }
+        int64_t w = 0;
+        for (int64_t i = 0; i < N; ++i) {
+            if (typ != 0 && type_h[i] != typ) continue;
+            if (out) out[w] = v[3 * i + which];
+            ++w;
+        }
+        if (count) *count = w;
+        return FCC_OK;
+    }
+
+    fcc_status body_energy(double* out) override {
+        std::vector<T> e;
+        FCC_TRY(fetch(E.p, (size_t)N, e));
+        FCC_TRY(sync_stream());
+        double acc = 0;
+        for (T v : e) acc += (double)v;
+        *out = acc;
+        return FCC_OK;
+    }
+
+    fcc_status timing(double* ms, int64_t* launches, int64_t* steps) override {
+        if (ms) *ms = last_ms;
+        if (launches) *launches = last_launches;
+        if (steps) *steps = last_steps;
+        return FCC_OK;
+    }
+};
+
+// ------------------------------------------------- stateless entry points
+template <class T>
+fcc_status build_neighbors_t(int64_t n, const double* x, const double* y, const double* rmax, double Lx, double Ly,
+                             double cutoff, double range, int32_t cap, int32_t* cellid_o, int32_t* perm_o,
+                             int32_t* start_o, int32_t* stop_o, int32_t* idx_o, int32_t* count_o) {
+    if (n < 0 || cap < 1) return fail(FCC_ERR_ARGUMENT, "n must be >= 0 and cap >= 1");
+    if (n == 0) return FCC_OK;
+    if (n > (1 << 27)) return fail(FCC_ERR_UNSUPPORTED, "at most 2^27 bodies");
+    cudaStream_t st;
+    CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+    } guard{st};
+    SimDesc<T> s{};
+    s.Lx = (T)Lx;
+    s.Ly = (T)Ly;
+    auto ncells = [&](T L) {
+        int64_t m = (int64_t)std::floor((double)L / cutoff);
+        return (int)(m >= 3 ? m : 1);
+    };
+    const int ncx = ncells(s.Lx), ncy = ncells(s.Ly);
+    if ((int64_t)ncx * ncy > (1 << 28)) return fail(FCC_ERR_UNSUPPORTED, "cell grid too large");
+    s.wx = s.Lx / (T)ncx;
+    s.wy = s.Ly / (T)ncy;
+    s.ncx = ncx;
+    s.ncy = ncy;
+    s.ncells = ncx * ncy;
+    s.n = (int)n;
+    s.nbrange = (T)range;
+    s.skin = T(0);
+    const size_t N = (size_t)n, C = (size_t)ncx * ncy;
+    DBuf<SimDesc<T>> sims;
+    DBuf<T> rec, xd, yd, rd;
+    DBuf<int> sim_of, cellid, slot, perm, cstart, cstop, ccount, cell_sim, nb_idx, nb_count, flags, maxcount;
+    DBuf<long long> clock, builds;
+    DBuf<GridSync> sync;
+    FCC_TRY(sims.upload(std::vector<SimDesc<T>>{s}, st));
+    std::vector<T> hx(N), hy(N), hr(N);
+    for (size_t i = 0; i < N; ++i) hx[i] = (T)x[i], hy[i] = (T)y[i], hr[i] = (T)rmax[i];
+    FCC_TRY(xd.upload(hx, st));
+    FCC_TRY(yd.upload(hy, st));
+    FCC_TRY(rd.upload(hr, st));
+    FCC_TRY(rec.alloc(N * RECW, st));
+    FCC_TRY(sim_of.alloc(N, st));
+    FCC_TRY(cellid.alloc(N, st));
+    FCC_TRY(slot.alloc(N, st));
+    FCC_TRY(perm.alloc(N, st));
+    FCC_TRY(cstart.alloc(C, st));
+    FCC_TRY(cstop.alloc(C, st));
+    FCC_TRY(ccount.alloc(C, st));
+    FCC_TRY(cell_sim.alloc(C, st));
+    FCC_TRY(nb_idx.alloc(N * cap, st));
+    FCC_TRY(nb_count.alloc(N, st));
+    FCC_TRY(flags.upload(std::vector<int>{F_ACTIVE | F_CONTACT | F_NEED}, st));
+    FCC_TRY(maxcount.alloc(1, st));
+    FCC_TRY(clock.alloc(1, st));
+    FCC_TRY(builds.alloc(1, st));
+    FCC_TRY(sync.upload(std::vector<GridSync>{GridSync{0, 0, 0, 1}}, st));
+    DevPtrs<T> d{};
+    d.sims = sims.p;
+    d.nsims = 1;
+    d.Ntot = (int)N;
+    d.Ctot = (int)C;
+    d.cap = cap;
+    d.sim_of = sim_of.p;
+    d.rec0 = rec.p;
+    d.rec1 = rec.p;
+    d.cellid = cellid.p;
+    d.slot = slot.p;
+    d.perm = perm.p;
+    d.cstart = cstart.p;
+    d.cstop = cstop.p;
+    d.ccount = ccount.p;
+    d.cell_sim = cell_sim.p;
+    d.nb_idx = nb_idx.p;
+    d.nb_count = nb_count.p;
+    d.flags = flags.p;
+    d.maxcount = maxcount.p;
+    d.clock = clock.p;
+    d.builds = builds.p;
+    d.sync = sync.p;
+    const int grid = (int)((N + 255) / 256);
+    k_pack_head<T><<<grid, 256, 0, st>>>(rec.p, xd.p, yd.p, rd.p, (int)N);
+    k_phase_count<T><<<grid, 256, 0, st>>>(d);
+    k_phase_scan<T><<<1, 1024, 0, st>>>(d);
+    k_phase_scatter<T><<<grid, 256, 0, st>>>(d);
+    k_phase_sort<T><<<(int)((C + 255) / 256), 256, 0, st>>>(d);
+    k_phase_neighbors<T><<<grid, 256, 0, st>>>(d);
+    CUDA_TRY(cudaGetLastError());
+    std::vector<int> a, b, cnt;
+    a.resize(N);
+    CUDA_TRY(cudaMemcpyAsync(a.data(), cellid.p, N * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < N; ++i) cellid_o[i] = a[i] + 1;
+    CUDA_TRY(cudaMemcpyAsync(a.data(), perm.p, N * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < N; ++i) perm_o[i] = a[i] + 1;
+    a.resize(C);
+    b.resize(C);
+    CUDA_TRY(cudaMemcpyAsync(a.data(), cstart.p, C * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(b.data(), cstop.p, C * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    for (size_t c = 0; c < C; ++c) {
+        const bool empty = b[c] <= a[c];
+        start_o[c] = empty ? 1 : a[c] + 1;
+        stop_o[c] = empty ? 0 : b[c];
+    }
+    cnt.resize(N);
+    a.resize(N * cap);
+    CUDA_TRY(cudaMemcpyAsync(cnt.data(), nb_count.p, N * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(a.data(), nb_idx.p, N * cap * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < N; ++i) {
+        count_o[i] = cnt[i];
+        for (int q = 0; q < cap; ++q) idx_o[i * cap + q] = q < cnt[i] ? a[i * cap + q] + 1 : 0;
+    }
+    return FCC_OK;
+}
+
+}  // namespace
+
+struct fcc_sim {
+    std::unique_ptr<EngineBase> impl;
+    int device = 0;
+};
+
+extern "C" {
+
+fcc_status fcc_create(const fcc_params* params, const fcc_bodies_host* bodies, fcc_sim** out) {
+    if (!out) return fail(FCC_ERR_ARGUMENT, "null output handle");
+    *out = nullptr;
+    if (!params) return fail(FCC_ERR_ARGUMENT, "null params");
+    std::unique_ptr<fcc_sim> h(new fcc_sim);
+    fcc_status st;
+    if (params->precision == 64) {
+        auto e = std::make_unique<Engine<double>>();
+        st = e->init(params, bodies);
+        h->impl = std::move(e);
+    } else if (params->precision == 32) {
+        auto e = std::make_unique<Engine<float>>();
+        st = e->init(params, bodies);
+        h->impl = std::move(e);
+    } else {
+        return fail(FCC_ERR_ARGUMENT, "precision must be 32 or 64");
+    }
+    if (st != FCC_OK) return st;
+    cudaGetDevice(&h->device);
+    *out = h.release();
+    return FCC_OK;
+}
+
+fcc_status fcc_destroy(fcc_sim* sim) {
+    if (sim) cudaSetDevice(sim->device);
+    delete sim;
+    return FCC_OK;
+}
+
+#define SIM_CALL(expr)                                                   \
+    do {                                                                 \
+        if (!sim) return fail(FCC_ERR_ARGUMENT, "null simulation");      \
+        cudaError_t e_ = cudaSetDevice(sim->device);                     \
+        if (e_ != cudaSuccess) return cuda_fail(e_, "cudaSetDevice");    \
+        return sim->impl->expr;                                          \
+    } while (0)
+
+fcc_status fcc_step(fcc_sim* sim, int64_t n) { SIM_CALL(step(n, true)); }
+fcc_status fcc_run(fcc_sim* sim, int64_t n, int64_t every, fcc_callback cb, void* user, int32_t graph) {
+    SIM_CALL(run(sim, n, every, cb, user, graph != 0));
+}
+fcc_status fcc_update_neighbors(fcc_sim* sim, int32_t force) { SIM_CALL(update_neighbors(force != 0)); }
+fcc_status fcc_compute_gradients(fcc_sim* sim) { SIM_CALL(compute_gradients()); }
+fcc_status fcc_get_state(fcc_sim* sim, fcc_bodies_host* out, int64_t* clock, double* t, int64_t* step) {
+    SIM_CALL(get_state(out, clock, t, step));
+}
+fcc_status fcc_set_state(fcc_sim* sim, const fcc_bodies_host* in, int64_t clock) { SIM_CALL(set_state(in, clock)); }
+fcc_status fcc_set_dt(fcc_sim* sim, double dt) { SIM_CALL(set_dt(dt)); }
+fcc_status fcc_get_gradients(fcc_sim* sim, const fcc_gradients_host* out) { SIM_CALL(get_gradients(out)); }
+fcc_status fcc_get_geometry(fcc_sim* sim, const fcc_geometry_host* out) { SIM_CALL(get_geometry(out)); }
+fcc_status fcc_neighbor_dims(fcc_sim* sim, int32_t* ncx, int32_t* ncy, int32_t* cap, int64_t* builds, int32_t* valid) {
+    SIM_CALL(neighbor_dims(ncx, ncy, cap, builds, valid));
+}
+fcc_status fcc_get_neighbors(fcc_sim* sim, const fcc_neighbors_host* out) { SIM_CALL(get_neighbors(out)); }
+fcc_status fcc_perimeters(fcc_sim* sim, int32_t type, double* out, int64_t* count) { SIM_CALL(observable(0, type, out, count)); }
+fcc_status fcc_areas(fcc_sim* sim, int32_t type, double* out, int64_t* count) { SIM_CALL(observable(1, type, out, count)); }
+fcc_status fcc_shape_index(fcc_sim* sim, int32_t type, double* out, int64_t* count) { SIM_CALL(observable(2, type, out, count)); }
+fcc_status fcc_body_energy(fcc_sim* sim, double* out) { SIM_CALL(body_energy(out)); }
+fcc_status fcc_last_timing(fcc_sim* sim, double* ms, int64_t* launches, int64_t* steps) {
+    SIM_CALL(timing(ms, launches, steps));
+}
+
+fcc_status fcc_philox_noise(uint64_t seed, uint64_t draw, int64_t nbodies, int32_t precision, double* out) {
+    if (precision != 32 && precision != 64) return fail(FCC_ERR_ARGUMENT, "precision must be 32 or 64");
+    if (nbodies <= 0) return FCC_OK;
+    if (nbodies > (1ll << 30)) return fail(FCC_ERR_UNSUPPORTED, "at most 2^30 bodies");
+    const uint32_t k0 = (uint32_t)(seed & 0xffffffffu), k1 = (uint32_t)(seed >> 32);
+    const size_t n3 = 3 * (size_t)nbodies;
+    const int grid = (int)((nbodies + 255) / 256);
+    if (precision == 64) {
+        double* d = nullptr;
+        CUDA_TRY(cudaMalloc(&d, n3 * sizeof(double)));
+        k_noise<double><<<grid, 256>>>(k0, k1, draw, (int)nbodies, d);
+        cudaError_t e = cudaMemcpy(out, d, n3 * sizeof(double), cudaMemcpyDeviceToHost);
+        cudaFree(d);
+        CUDA_TRY(e);
+    } else {
+        float* d = nullptr;
+        CUDA_TRY(cudaMalloc(&d, n3 * sizeof(float)));
+        k_noise<float><<<grid, 256>>>(k0, k1, draw, (int)nbodies, d);
+        std::vector<float> h(n3);
+        cudaError_t e = cudaMemcpy(h.data(), d, n3 * sizeof(float), cudaMemcpyDeviceToHost);
+        cudaFree(d);
+        CUDA_TRY(e);
+        for (size_t q = 0; q < n3; ++q) out[q] = (double)h[q];
+    }
+    return FCC_OK;
+}
+
+fcc_status fcc_build_neighbors(int32_t precision, int64_t n, const double* x, const double* y, const double* rmax,
+                               double Lx, double Ly, double cutoff, double range, int32_t cap, int32_t* cellid,
+                               int32_t* perm, int32_t* start, int32_t* stop, int32_t* idx, int32_t* count) {
+    if (precision == 64)
+        return build_neighbors_t<double>(n, x, y, rmax, Lx, Ly, cutoff, range, cap, cellid, perm, start, stop, idx, count);
+    if (precision == 32)
+        return build_neighbors_t<float>(n, x, y, rmax, Lx, Ly, cutoff, range, cap, cellid, perm, start, stop, idx, count);
+    return fail(FCC_ERR_ARGUMENT, "precision must be 32 or 64");
+}
+
+const char* fcc_last_error(void) { return g_err.c_str(); }
+
+const char* fcc_version(void) {
+    return "libfcc_b200 sm_100a: persistent cooperative step kernel, 8 lanes x 5 nodes per body";
+}
+
+}  // extern "C"

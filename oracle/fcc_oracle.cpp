@@ -93,8 +93,9 @@ template <class T> inline T wrap(T x, T L, int32_t& shift) {
 
 // src/neighbors.jl:40-42
 template <class T> inline void grid_coords(int32_t ncx, int32_t ncy, T wx, T wy, T x, T y, int32_t& cx, int32_t& cy) {
-    cx = std::min((int32_t)(x / wx), ncx - 1);
-    cy = std::min((int32_t)(y / wy), ncy - 1);
+    // clamped into the grid (inputs outside [0, L) would index outside it)
+    cx = std::max<int32_t>(0, std::min((int32_t)(x / wx), ncx - 1));
+    cy = std::max<int32_t>(0, std::min((int32_t)(y / wy), ncy - 1));
 }
 
 inline int32_t jmod(int32_t a, int32_t n) {
@@ -221,6 +222,11 @@ template <class T> struct Sim final : SimBase {
         }
         N = b->n;
         if (N < 0) return fail(FCC_ERR_DIMENSION, "inconsistent body array lengths");
+        int32_t maxtype = 0;
+        for (int64_t i = 0; i < N; ++i) maxtype = std::max(maxtype, b->type[i]);
+        for (const Term<T>& tm : contact_terms)
+            if (tm.kind == FCC_OVERLAP && tm.nJ > 1 && tm.nJ < maxtype)
+                return fail(FCC_ERR_DIMENSION, "Overlap coupling table smaller than the number of body types");
         for (int64_t i = 0; i < N; ++i)
             if (b->type[i] > p->ntypes) return fail(FCC_ERR_ARGUMENT, "body type without BodyType entry");
         for (int64_t i = 0; i < N; ++i)
@@ -587,8 +593,9 @@ template <class T> struct Sim final : SimBase {
             T g = 0;
             if (tm.applies(ti)) {
                 if (tm.kind == FCC_OVERLAP) {
+                    // a 1 x 1 table (scalar coupling) applies to every type pair
                     int nJ = tm.nJ;
-                    size_t ij = (size_t)(ti - 1) + (size_t)nJ * (tj - 1);
+                    size_t ij = nJ == 1 ? 0 : (size_t)(ti - 1) + (size_t)nJ * (tj - 1);
                     T J = rel ? tm.Jrel[ij] : tm.J[ij];
                     g = d >= 0 ? J : T(0);
                 } else {
