@@ -252,6 +252,17 @@ __device__ __forceinline__ long long ldcg(const long long* p) { return __ldcg(p)
 __device__ __forceinline__ float4 ldcg(const float4* p) { return __ldcg(p); }
 __device__ __forceinline__ double2 ldcg(const double2* p) { return __ldcg(p); }
 
+// ------------------------------------------------------------ async copies
+// 16-byte global -> shared copies that bypass L1 (cp.async.cg): the
+// neighbour records a body needs are staged in shared memory while the warp
+// synthesises its own contour.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // ------------------------------------------------------------ grid barrier
 // Barrier over all blocks of a cooperative launch (all co-resident).  Arrival
 // is an acq_rel atomic, the release a release store, the wait an acquire

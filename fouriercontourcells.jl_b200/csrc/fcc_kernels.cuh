@@ -251,6 +251,43 @@ __device__ void phase_neighbors(const DevPtrs<T>& d, int tid, int nthr) {
 }
 
 // ============================================================= update ==
+// Neighbour records staged in shared memory per body (the rest are read from
+// L2 in the loop).  At packing 0.95 with the 0.3 skin a body lists 6-9.
+constexpr int NBMAX = 12;
+
+template <class T, int L>
+__host__ __device__ constexpr size_t stage_bytes_per_warp() {
+    return (size_t)(32 / L) * NBMAX * RECW * sizeof(T);
+}
+
+// Operands of the update loaded early (their latency overlaps the force
+// evaluation): the body's a0, its lane's shape modes and, on lane 0, the
+// skin reference of the last neighbour-list build.
+template <class T, int L>
+struct UpdatePre {
+    static constexpr int MPL = (KM + L - 1) / L;
+    T a0, a[MPL], b[MPL], x0, y0, rmax0;
+};
+
+template <class T, int L>
+__device__ __forceinline__ void load_update_pre(const DevPtrs<T>& d, int gg, int l, int K, UpdatePre<T, L>& u) {
+    const T* cf = d.coef + (size_t)gg * NCM;
+    u.a0 = ldcg(cf);
+#pragma unroll
+    for (int v = 0; v < UpdatePre<T, L>::MPL; ++v) {
+        const int m = l + v * L;
+        u.a[v] = m < K ? ldcg(cf + 1 + m) : T(0);
+        u.b[v] = m < K ? ldcg(cf + 1 + KM + m) : T(0);
+    }
+    if (l == 0) {
+        u.x0 = ldcg(d.x0 + gg);
+        u.y0 = ldcg(d.y0 + gg);
+        u.rmax0 = ldcg(d.rmax0 + gg);
+    } else {
+        u.x0 = u.y0 = u.rmax0 = T(0);
+    }
+}
+
 // Translational displacement of a body with substrate drag, plus the forces
 // of its children with parent drag (src/dynamics.jl:84-99).
 template <class T>
@@ -285,9 +322,9 @@ __device__ __forceinline__ void substrate_displacement(const DevPtrs<T>& d, cons
 template <class T, int L>
 __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T>& P, bool act, int g, int s, int l,
                                             long long clk, const T (&rv)[RECW], T r0, int ti, T fx, T fy, T tt,
-                                            const T (&gl)[NCM], bool split) {
+                                            const T (&gl)[NCM], const UpdatePre<T, L>& pre, bool split) {
     constexpr unsigned FULL = 0xffffffffu;
-    constexpr int MPL = (KM + L - 1) / L;
+    constexpr int MPL = UpdatePre<T, L>::MPL;
     const T dt = P.dt;
     const T tho = rv[R_TH];
     const uint32_t li = (uint32_t)(g - P.body_off + 1);
@@ -301,7 +338,7 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
     const T thn = tho - (dt * P.muth[ti]) * tt + sig_r * z3;
 
     T* cf = d.coef + (size_t)(act ? g : 0) * NCM;
-    const T a0 = ldcg(cf);
+    const T a0 = pre.a0;
     const T ga0 = r0 * gl[0];
     const T dtmu = dt * P.muab[ti];
     const int K = P.K;
@@ -321,7 +358,7 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
             gb *= r0;
             T so, co;
             t_sincos(T(m + 2) * tho, &so, &co);
-            const T a = ldcg(cf + 1 + m), b = ldcg(cf + 1 + KM + m);
+            const T a = pre.a[u], b = pre.b[u];
             const T gca = ga * co + gb * so - ga0 * a / (T(2) * a0);
             const T gcb = -ga * so + gb * co - ga0 * b / (T(2) * a0);
             an[u] = a - dtmu * gca;
@@ -409,9 +446,9 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
         const int f = ldcg(d.flags + s);
         // skin check of the new state (src/neighbors.jl:198-205)
         if ((f & F_CONTACT) && (f & F_VALID) && P.skin > T(0)) {
-            const T dx = minimum_image_exact(sub_rn(xw, ldcg(d.x0 + g)), P.Lx);
-            const T dy = minimum_image_exact(sub_rn(yw, ldcg(d.y0 + g)), P.Ly);
-            const T grow = sub_rn(rmax, ldcg(d.rmax0 + g));
+            const T dx = minimum_image_exact(sub_rn(xw, pre.x0), P.Lx);
+            const T dy = minimum_image_exact(sub_rn(yw, pre.y0), P.Ly);
+            const T grow = sub_rn(rmax, pre.rmax0);
             const T delta = add_rn(t_sqrt(add_rn(mul_rn(dx, dx), mul_rn(dy, dy))), grow > T(0) ? grow : T(0));
             if (mul_rn(T(2), delta) > P.skin) atomicOr(&d.flags[s], F_REBUILD);
         }
@@ -423,7 +460,8 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
 enum : int { MODE_FUSED = 0, MODE_FORCES = 1, MODE_DIAG = 2 };
 
 // Forces on the 32/L bodies of warp group `wg`, and in MODE_FUSED their
-// update.  Follows, per body i:
+// update.  `stage` is this warp's shared-memory slot for neighbour records.
+// Follows, per body i:
 //   contour synthesis R, R' at the nodes        src/geometry.jl:248-257
 //   body terms (Tension, PerimeterElasticity)   src/gradients.jl:70-98, 197-228
 //   contact pressure at the nodes (Overlap,     src/energies/contact.jl:300-324,
@@ -431,9 +469,10 @@ enum : int { MODE_FUSED = 0, MODE_FORCES = 1, MODE_DIAG = 2 };
 //   bond forces                                 src/energies/bonds.jl:98-111
 //   pullback glab = S' Gall                     src/gradients.jl:374-386
 template <class T, int L, int S, bool ONE, int MODE>
-__device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg) {
+__device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stage) {
     constexpr int BPW = 32 / L;
     constexpr unsigned FULL = 0xffffffffu;
+    constexpr int CH16 = RECW * (int)sizeof(T) / 16;  // 16-byte chunks per record
     const int lane = threadIdx.x & 31;
     const int l = lane & (L - 1);
     const int g = wg * BPW + lane / L;
@@ -448,12 +487,37 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg) {
     const int nth = P.nth;
     const T dphi = P.dphi;
 
+    // ---- early loads: own record, neighbour list, staged neighbour records, update operands
     T rv[RECW];
     load_rec(rc + (size_t)gg * RECW, rv);
+    const T r0 = __ldg(d.R0 + gg);
+    const bool contact = act && (fl & F_CONTACT);
+    const int cnt = contact ? min(ldcg(d.nb_count + gg), d.cap) : 0;
+    T* snb = stage + (size_t)(lane / L) * NBMAX * RECW;
+    // stage the records of neighbours [base, base + NBMAX) of this body
+    auto stage_batch = [&](int base) {
+        const int npre = min(cnt - base, NBMAX);
+        __syncwarp();  // every lane is done with the previous contents
+#pragma unroll
+        for (int u = 0; u < (NBMAX + L - 1) / L; ++u) {
+            const int q = l + u * L;
+            if (q < npre) {
+                const int j = ldcg(d.nb_idx + (size_t)gg * d.cap + base + q);
+                const T* src = rc + (size_t)j * RECW;
+#pragma unroll
+                for (int c = 0; c < CH16; ++c) cp_async16(snb + q * RECW + c * (16 / sizeof(T)), src + c * (16 / sizeof(T)));
+            }
+        }
+        cp_async_commit();
+    };
+    stage_batch(0);
+    int staged_base = 0;
+    UpdatePre<T, L> pre;
+    if (MODE == MODE_FUSED) load_update_pre(d, gg, l, P.K, pre);
+
     const int wv = unpack_w(rv[R_W]);
     const int ti = wv & 7;
     const int pi = wv >> 3;
-    const T r0 = __ldg(d.R0 + gg);
 
     T R[S], R1[S], C1[S], S1[S];
     unsigned vmask = 0;
@@ -520,8 +584,8 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg) {
 #pragma unroll
     for (int r = 0; r < NCM; ++r) gl[r] = T(0);
 
-    const bool contact = act && (fl & F_CONTACT);
-    const int cnt = contact ? min(ldcg(d.nb_count + gg), d.cap) : 0;
+    cp_async_wait_all();
+    __syncwarp();
     const int maxc = __reduce_max_sync(FULL, cnt);
     const T xi = rv[R_X], yi = rv[R_Y];
     const T Lx = P.Lx, Ly = P.Ly, iLx = P.invLx, iLy = P.invLy, crange = P.crange;
@@ -539,69 +603,75 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg) {
                 rcx[sl] = R[sl] * C1[sl];
                 rcy[sl] = R[sl] * S1[sl];
             }
-            for (int q = 0; q < maxc; ++q) {
-                const bool qa = q < cnt;
-                const int j = qa ? ldcg(d.nb_idx + (size_t)gg * d.cap + q) : gg;
-                T xj, yj, rmj, wj;
-                load_head(rc + (size_t)j * RECW, xj, yj, rmj, wj);
-                const T dxc = minimum_image_fast(xi - xj, Lx, iLx);
-                const T dyc = minimum_image_fast(yi - yj, Ly, iLy);
-                const T lim = rmj + crange;
-                const T lim2 = lim * lim;
-                unsigned hm = 0;
-                if (qa) {
-#pragma unroll
-                    for (int sl = 0; sl < S; ++sl) {
-                        T dx = rcx[sl] + dxc, dy = rcy[sl] + dyc;
-                        if (rewrap) {
-                            dx = minimum_image_fast(dx, Lx, iLx);
-                            dy = minimum_image_fast(dy, Ly, iLy);
-                        }
-                        if ((vmask & (1u << sl)) && dx * dx + dy * dy <= lim2) hm |= 1u << sl;
-                    }
+            for (int base = 0; base < maxc; base += NBMAX) {
+                if (base != staged_base) {  // lists longer than the stage: restage
+                    stage_batch(base);
+                    cp_async_wait_all();
+                    __syncwarp();
+                    staged_base = base;
                 }
-                // one hit per lane per round: the hit path runs as many rounds as
-                // the busiest lane has hits for this neighbour (usually one)
-                while (__any_sync(FULL, hm != 0)) {
-                    if (hm) {
-                        const int sl = __ffs(hm) - 1;
-                        hm &= hm - 1;
-                        T rx = rcx[0], ry = rcy[0];
+                const int qn = min(maxc - base, NBMAX);
+                for (int qq = 0; qq < qn; ++qq) {
+                    const bool qa = base + qq < cnt;
+                    const T* nrec = snb + qq * RECW;
+                    const T xj = nrec[R_X], yj = nrec[R_Y], rmj = nrec[R_RMAX], wj = nrec[R_W];
+                    const T dxc = minimum_image_fast(xi - xj, Lx, iLx);
+                    const T dyc = minimum_image_fast(yi - yj, Ly, iLy);
+                    const T lim = rmj + crange;
+                    const T lim2 = lim * lim;
+                    unsigned hm = 0;
+                    if (qa) {
 #pragma unroll
-                        for (int u = 1; u < S; ++u)
-                            if (sl == u) rx = rcx[u], ry = rcy[u];
-                        T dx = rx + dxc, dy = ry + dyc;
-                        if (rewrap) {
-                            dx = minimum_image_fast(dx, Lx, iLx);
-                            dy = minimum_image_fast(dy, Ly, iLy);
+                        for (int sl = 0; sl < S; ++sl) {
+                            T dx = rcx[sl] + dxc, dy = rcy[sl] + dyc;
+                            if (rewrap) {
+                                dx = minimum_image_fast(dx, Lx, iLx);
+                                dy = minimum_image_fast(dy, Ly, iLy);
+                            }
+                            if ((vmask & (1u << sl)) && dx * dx + dy * dy <= lim2) hm |= 1u << sl;
                         }
-                        const T dist = t_sqrt(dx * dx + dy * dy);
-                        T cp = T(1), sp = T(0);
-                        if (dist > T(0)) {
-                            const T inv = T(1) / dist;
-                            cp = dx * inv;
-                            sp = dy * inv;
-                        }
-                        T lj[20];
-                        load_lab(rc + (size_t)j * RECW, lj);
-                        // R_j(psi) by the angle-addition recurrence (src/geometry.jl:282-291)
-                        T c = cp, sn = sp, rj = lj[0];
+                    }
+                    // one hit per lane per round: the hit path runs as many rounds as
+                    // the busiest lane has hits for this neighbour (usually one)
+                    while (__any_sync(FULL, hm != 0)) {
+                        if (hm) {
+                            const int sl = __ffs(hm) - 1;
+                            hm &= hm - 1;
+                            T rx = rcx[0], ry = rcy[0];
 #pragma unroll
-                        for (int m = 0; m < KM; ++m) {
-                            const T cn = c * cp - sn * sp;
-                            sn = sn * cp + c * sp;
-                            c = cn;
-                            rj += lj[1 + m] * c + lj[1 + KM + m] * sn;
-                        }
-                        const T dd = rj - dist;
-                        const int wjv = unpack_w(wj);
-                        const int tj = wjv & 7;
-                        const int rel = (wjv >> 3) == pi ? 1 : 0;
-                        T gv = dd >= T(0) ? P.cA[rel][ti][tj] : T(0);
-                        if (dd > T(0)) gv += P.cB[ti] * dd;
+                            for (int u = 1; u < S; ++u)
+                                if (sl == u) rx = rcx[u], ry = rcy[u];
+                            T dx = rx + dxc, dy = ry + dyc;
+                            if (rewrap) {
+                                dx = minimum_image_fast(dx, Lx, iLx);
+                                dy = minimum_image_fast(dy, Ly, iLy);
+                            }
+                            const T dist = t_sqrt(dx * dx + dy * dy);
+                            T cp = T(1), sp = T(0);
+                            if (dist > T(0)) {
+                                const T inv = T(1) / dist;
+                                cp = dx * inv;
+                                sp = dy * inv;
+                            }
+                            // R_j(psi) by the angle-addition recurrence (src/geometry.jl:282-291)
+                            T c = cp, sn = sp, rj = nrec[R_A0];
 #pragma unroll
-                        for (int u = 0; u < S; ++u)
-                            if (sl == u) p[u] += gv;
+                            for (int m = 0; m < KM; ++m) {
+                                const T cn = c * cp - sn * sp;
+                                sn = sn * cp + c * sp;
+                                c = cn;
+                                rj += nrec[R_AL + m] * c + nrec[R_BE + m] * sn;
+                            }
+                            const T dd = rj - dist;
+                            const int wjv = unpack_w(wj);
+                            const int tj = wjv & 7;
+                            const int rel = (wjv >> 3) == pi ? 1 : 0;
+                            T gv = dd >= T(0) ? P.cA[rel][ti][tj] : T(0);
+                            if (dd > T(0)) gv += P.cB[ti] * dd;
+#pragma unroll
+                            for (int u = 0; u < S; ++u)
+                                if (sl == u) p[u] += gv;
+                        }
                     }
                 }
             }
@@ -722,7 +792,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg) {
         d.gth[g] = tt;
         d.E[g] = E;
     }
-    update_body<T, L>(d, P, act, g, s, l, clk, rv, r0, ti, fx, fy, tt, gl, false);
+    update_body<T, L>(d, P, act, g, s, l, clk, rv, r0, ti, fx, fy, tt, gl, pre, false);
 }
 
 // Phase B of the split step: displacement with parent drag + update of the
@@ -744,11 +814,13 @@ __device__ __forceinline__ void update_warp_split(const DevPtrs<T>& d, int wg) {
     load_rec(rec_cur(d, clk) + (size_t)gg * RECW, rv);
     const int ti = unpack_w(rv[R_W]) & 7;
     const T r0 = __ldg(d.R0 + gg);
+    UpdatePre<T, L> pre;
+    load_update_pre(d, gg, l, P.K, pre);
     T gl[NCM];
 #pragma unroll
     for (int r = 0; r < NCM; ++r) gl[r] = ldcg(d.glab + (size_t)gg * NCM + r);
     const T fx = ldcg(d.gx + gg), fy = ldcg(d.gy + gg), tt = ldcg(d.gth + gg);
-    update_body<T, L>(d, P, act, g, s, l, clk, rv, r0, ti, fx, fy, tt, gl, true);
+    update_body<T, L>(d, P, act, g, s, l, clk, rv, r0, ti, fx, fy, tt, gl, pre, true);
 }
 
 // Last block of a step's closing barrier: tick the clocks of the simulations
@@ -794,23 +866,33 @@ __device__ __forceinline__ bool rebuild_prologue(const DevPtrs<T>& d, int tid, i
     return grid_barrier(d.sync, noop);
 }
 
+// Dynamic shared memory of the force kernels: one neighbour stage per warp.
+template <class T>
+__device__ __forceinline__ T* warp_stage(size_t bytes_per_warp) {
+    extern __shared__ __align__(16) unsigned char fcc_smem[];
+    return reinterpret_cast<T*>(fcc_smem + (threadIdx.x >> 5) * bytes_per_warp);
+}
+
 // Persistent cooperative step kernel: `nsteps` whole time steps per launch.
-template <class T, int L, int S, bool ONE, bool SPLIT>
-__global__ void __launch_bounds__(256) k_step(DevPtrs<T> d, int nsteps) {
-    const int wpb = blockDim.x >> 5;
-    const int wid = blockIdx.x * wpb + (threadIdx.x >> 5);
-    const int nwarps = gridDim.x * wpb;
+// Each block takes a contiguous range of warp groups (balanced bodies per SM).
+template <class T, int L, int S, bool ONE, bool SPLIT, int BLK>
+__global__ void __launch_bounds__(BLK) k_step(DevPtrs<T> d, int nsteps) {
+    constexpr int WPB = BLK / 32;
+    const int warp = threadIdx.x >> 5;
     const int ngroups = (d.Ntot + (32 / L) - 1) / (32 / L);
+    const int g0 = (int)((long long)ngroups * blockIdx.x / gridDim.x);
+    const int g1 = (int)((long long)ngroups * (blockIdx.x + 1) / gridDim.x);
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nthr = gridDim.x * blockDim.x;
+    T* stage = warp_stage<T>(stage_bytes_per_warp<T, L>());
     for (int st = 0; st < nsteps; ++st) {
         if (ld_acquire(&d.sync->any_need))
             if (!rebuild_prologue(d, tid, nthr)) return;
-        for (int wg = wid; wg < ngroups; wg += nwarps)
-            forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg);
+        for (int wg = g0 + warp; wg < g1; wg += WPB)
+            forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage);
         if (SPLIT) {
             if (!grid_barrier(d.sync, [] {})) return;
-            for (int wg = wid; wg < ngroups; wg += nwarps) update_warp_split<T, L>(d, wg);
+            for (int wg = g0 + warp; wg < g1; wg += WPB) update_warp_split<T, L>(d, wg);
         }
         if (!grid_barrier(d.sync, [&] { bookkeeping(d); })) return;
     }
@@ -823,7 +905,8 @@ __global__ void __launch_bounds__(256) k_gradients(DevPtrs<T> d) {
     const int wpb = blockDim.x >> 5;
     const int wg = blockIdx.x * wpb + (threadIdx.x >> 5);
     const int ngroups = (d.Ntot + (32 / L) - 1) / (32 / L);
-    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG>(d, wg);
+    T* stage = warp_stage<T>(stage_bytes_per_warp<T, L>());
+    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG>(d, wg, stage);
 }
 
 // Stand-alone rebuild phases (update_neighbors!, and the stateless neighbour

@@ -457,25 +457,28 @@ struct Engine final : EngineBase {
         return sync_stream();
     }
 
-    template <class F>
-    fcc_status occupancy(F kernel, int& blocks) {
-        int per_sm = 0;
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, BLOCK, 0));
-        if (per_sm < 1) return fail(FCC_ERR_UNSUPPORTED, "step kernel does not fit on an SM");
-        blocks = per_sm * nsm;
-        return FCC_OK;
+    static constexpr size_t stage_bytes() { return (size_t)(BLOCK / 32) * stage_bytes_per_warp<T, LANES>(); }
+
+    // the persistent step kernel variant for this simulation
+    void* step_kernel() const {
+        if (one_chunk())
+            return split ? (void*)k_step<T, LANES, SLOTS, true, true, BLOCK> : (void*)k_step<T, LANES, SLOTS, true, false, BLOCK>;
+        return split ? (void*)k_step<T, LANES, SLOTS, false, true, BLOCK> : (void*)k_step<T, LANES, SLOTS, false, false, BLOCK>;
+    }
+    void* grad_kernel() const {
+        return one_chunk() ? (void*)k_gradients<T, LANES, SLOTS, true> : (void*)k_gradients<T, LANES, SLOTS, false>;
     }
 
     bool one_chunk() const { return nth <= LANES * SLOTS; }
 
     fcc_status configure() {
-        int maxblocks = 0;
-        if (one_chunk())
-            FCC_TRY(split ? occupancy(k_step<T, LANES, SLOTS, true, true>, maxblocks)
-                          : occupancy(k_step<T, LANES, SLOTS, true, false>, maxblocks));
-        else
-            FCC_TRY(split ? occupancy(k_step<T, LANES, SLOTS, false, true>, maxblocks)
-                          : occupancy(k_step<T, LANES, SLOTS, false, false>, maxblocks));
+        const int smem = (int)stage_bytes();
+        for (void* fn : {step_kernel(), grad_kernel()})
+            CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        int per_sm = 0;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_kernel(), BLOCK, smem));
+        if (per_sm < 1) return fail(FCC_ERR_UNSUPPORTED, "step kernel does not fit on an SM");
+        const int maxblocks = per_sm * nsm;
         const int64_t groups = (N + (32 / LANES) - 1) / (32 / LANES);
         const int64_t want = std::max<int64_t>(1, (groups + BLOCK / 32 - 1) / (BLOCK / 32));
         step_grid = (int)std::min<int64_t>(want, maxblocks);
@@ -569,12 +572,7 @@ struct Engine final : EngineBase {
     fcc_status launch_steps(int nsteps) {
         DevPtrs<T> d = ptrs();
         void* args[] = {&d, &nsteps};
-        void* fn;
-        if (one_chunk())
-            fn = split ? (void*)k_step<T, LANES, SLOTS, true, true> : (void*)k_step<T, LANES, SLOTS, true, false>;
-        else
-            fn = split ? (void*)k_step<T, LANES, SLOTS, false, true> : (void*)k_step<T, LANES, SLOTS, false, false>;
-        CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(step_grid), dim3(BLOCK), args, 0, stream));
+        CUDA_TRY(cudaLaunchCooperativeKernel(step_kernel(), dim3(step_grid), dim3(BLOCK), args, stage_bytes(), stream));
         ++last_launches;
         return FCC_OK;
     }
@@ -680,11 +678,11 @@ struct Engine final : EngineBase {
         FCC_TRY(ensure_diag());
         const DevPtrs<T> d = ptrs();
         const int64_t groups = (N + (32 / LANES) - 1) / (32 / LANES);
-        const int grid = (int)((groups + BLOCK / 32 - 1) / (BLOCK / 32));
+        const int grid = (int)((groups + 256 / 32 - 1) / (256 / 32));
         if (one_chunk())
-            k_gradients<T, LANES, SLOTS, true><<<grid, BLOCK, 0, stream>>>(d);
+            k_gradients<T, LANES, SLOTS, true><<<grid, 256, stage_bytes(), stream>>>(d);
         else
-            k_gradients<T, LANES, SLOTS, false><<<grid, BLOCK, 0, stream>>>(d);
+            k_gradients<T, LANES, SLOTS, false><<<grid, 256, stage_bytes(), stream>>>(d);
         CUDA_TRY(cudaGetLastError());
         return sync_stream();
     }

@@ -159,7 +159,10 @@ def test_gradients_match_oracle_fp64(nθ):
         assert relerr(getattr(g.grad, f), getattr(o.grad, f)) < 1e-12, f
 
 
-def near_ties(o, thr=1e-4):
+def near_ties(o, thr=3e-6):
+    """Bodies with a node whose penetration depth |d| into a neighbour is
+    below `thr`: FP32 computes d to ~1e-6, so the Heaviside g = J H(d) may
+    legitimately flip there."""
     _, _, md = o.contact_counters()
     return md < thr
 
@@ -238,7 +241,10 @@ def test_two_discs_overlap_force_chunked():
     assert math.isclose(gr.gx[1], -math.sqrt(4 - d * d), rel_tol=1e-3)
     assert abs(gr.gy[0]) < 1e-6
     o = two_body((fcc.Overlap(1.0),), d=d, nθ=8000)
-    for f in ("gx", "gy", "gθ", "gcoef", "P"):
+    F = np.abs(o.grad.gx).max()  # gy and the torque vanish by symmetry: judge them on the force scale
+    for f in ("gx", "gy", "gθ"):
+        assert np.abs(getattr(gr, f) - getattr(o.grad, f)).max() < 1e-12 * F, f
+    for f in ("gcoef", "P", "GR"):
         assert relerr(getattr(gr, f), getattr(o.grad, f)) < 1e-12, f
 
 
@@ -293,9 +299,12 @@ def test_one_step_fp32_vs_fp64_oracle():
     o.step(1)
     bg, bo = g.bodies, o.bodies
     for f in ("x", "y", "θ", "coef"):
-        dg = getattr(bg, f) - getattr(b0, f)
-        do = getattr(bo, f) - getattr(b0, f)
-        assert relerr(dg, do, keep) < 1e-5, f
+        # the FP32 state resolves an increment only to the FP32 spacing of the
+        # state itself: 1e-5 of the increments' scale plus 2 ulp of the state
+        sg, so, s0 = getattr(bg, f), getattr(bo, f), getattr(b0, f)
+        dg, do = sg - s0, so - s0
+        tol = 1e-5 * np.abs(do).max() + 2 * np.spacing(np.abs(so).astype(np.float32)).astype(np.float64)
+        assert (np.abs(dg - do)[..., keep] <= tol[..., keep]).all(), f
 
 
 # ------------------------------------------------------------ trajectories
@@ -505,7 +514,7 @@ def test_n16384_fp32_forces_vs_oracle():
     g.refresh()
     o.refresh()
     keep = ~near_ties(o)
-    assert keep.mean() > 0.9
+    assert keep.mean() > 0.95
     for f in ("gx", "gy", "gθ", "gcoef", "Ebody"):
         assert relerr(getattr(g.grad, f), getattr(o.grad, f), keep) < 1e-5, f
 
