@@ -3,9 +3,9 @@
 // Layout in HBM (all bodies of all simulations of one engine, global body
 // index g; a single Simulation is an engine with one simulation):
 //
-//   rec[2][g][24]  geometry record, ping-pong by the parity of the
-//                  simulation's clock (current = clock & 1).  Neighbours
-//                  read it, so a step reads rec[cur] and writes rec[cur^1]:
+//   rec[2][g][24]  geometry record, ping-pong by the parity of the engine's
+//                  step counter (current = rec[par]).  Neighbours read it,
+//                  so a step reads rec[par] and writes rec[par^1]:
 //                    [0] x  [1] y  [2] rmax  [3] w = parent_global<<3 | (type-1)
 //                    [4] R0*a0  [5..13] R0*alpha_n  [14..22] R0*beta_n  [23] theta
 //                  (lab-frame coefficients scaled by R0, src/geometry.jl:208-227;
@@ -299,12 +299,12 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, F&& last) {
     unsigned gen = 0;
     if (threadIdx.x == 0) {
         gen = ld_acquire(&gs->gen);
-        unsigned prev = atom_add_acq_rel(&gs->count, 1u);
+        const unsigned prev = atom_add_acq_rel(&gs->count, 1u);
         s_last = (prev == gridDim.x - 1);
+        s_err = 0;
     }
     __syncthreads();
     if (s_last) {
-        __threadfence();
         last();
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -317,16 +317,19 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, F&& last) {
         while (ld_acquire(&gs->gen) == gen) {
             if (++it > SPIN_LIMIT) {
                 atomicExch(&gs->error, 1);
+                s_err = 1;
                 break;
             }
-            __nanosleep(32);
+            __nanosleep(20);
         }
     }
     __syncthreads();
-    __threadfence();
-    if (threadIdx.x == 0) s_err = ld_acquire(&gs->error);
-    __syncthreads();
     return s_err == 0;
 }
+
+// Fast reciprocal square root for the FP32 force path (rsqrt, ~2 ulp);
+// FP64 keeps the correctly rounded 1/sqrt.
+__device__ __forceinline__ float fast_rsqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double fast_rsqrt(double x) { return 1.0 / sqrt(x); }
 
 }  // namespace fcc

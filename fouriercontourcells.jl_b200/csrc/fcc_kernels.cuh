@@ -73,17 +73,56 @@ __device__ __forceinline__ void load_lab(const double* p, double (&c)[20]) {
     }
 }
 
+// The current record buffer is rec[par], par = parity of the engine's step
+// counter (all simulations of an engine advance together; a frozen one
+// copies its records forward).
 template <class T>
-__device__ __forceinline__ const T* rec_cur(const DevPtrs<T>& d, long long clk) {
-    return (clk & 1) ? d.rec1 : d.rec0;
+__device__ __forceinline__ const T* rec_cur(const DevPtrs<T>& d, int par) {
+    return par ? d.rec1 : d.rec0;
 }
 template <class T>
-__device__ __forceinline__ T* rec_next(const DevPtrs<T>& d, long long clk) {
-    return (clk & 1) ? d.rec0 : d.rec1;
+__device__ __forceinline__ T* rec_next(const DevPtrs<T>& d, int par) {
+    return par ? d.rec0 : d.rec1;
 }
 template <class T>
-__device__ __forceinline__ T* rec_cur_mut(const DevPtrs<T>& d, long long clk) {
-    return (clk & 1) ? d.rec1 : d.rec0;
+__device__ __forceinline__ T* rec_cur_mut(const DevPtrs<T>& d, int par) {
+    return par ? d.rec1 : d.rec0;
+}
+
+// shared-memory vector loads of staged records
+__device__ __forceinline__ float4 lds4(const float* p) {
+    float4 v;
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ void lds_head(const float* p, float& x, float& y, float& rm, float& w) {
+    const float4 v = lds4(p);
+    x = v.x, y = v.y, rm = v.z, w = v.w;
+}
+__device__ __forceinline__ void lds_head(const double* p, double& x, double& y, double& rm, double& w) {
+    x = p[R_X], y = p[R_Y], rm = p[R_RMAX], w = p[R_W];
+}
+__device__ __forceinline__ void lds_lab(const float* p, float (&c)[20]) {
+#pragma unroll
+    for (int u = 0; u < 5; ++u) {
+        const float4 v = lds4(p + R_A0 + 4 * u);
+        c[4 * u] = v.x, c[4 * u + 1] = v.y, c[4 * u + 2] = v.z, c[4 * u + 3] = v.w;
+    }
+}
+__device__ __forceinline__ void lds_lab(const double* p, double (&c)[20]) {
+#pragma unroll
+    for (int u = 0; u < 20; ++u) c[u] = p[R_A0 + u];
+}
+
+// |u| and 1/|u| of a contour node distance (FP32: one rsqrt)
+__device__ __forceinline__ void norm_inv(float x2, float& n, float& inv) {
+    inv = rsqrtf(x2);
+    n = x2 * inv;
+}
+__device__ __forceinline__ void norm_inv(double x2, double& n, double& inv) {
+    n = sqrt(x2);
+    inv = 1.0 / n;
 }
 
 __device__ __forceinline__ int jmod(int a, int n) {
@@ -104,12 +143,12 @@ __device__ __forceinline__ void grid_coords(const SimDesc<T>& P, T x, T y, int& 
 // loop over the bodies or cells of the simulations flagged F_NEED.
 
 template <class T>
-__device__ void phase_count(const DevPtrs<T>& d, int tid, int nthr) {
+__device__ void phase_count(const DevPtrs<T>& d, int par, int tid, int nthr) {
     for (int g = tid; g < d.Ntot; g += nthr) {
         const int s = __ldg(d.sim_of + g);
         if (!(ldcg(d.flags + s) & F_NEED)) continue;
         const SimDesc<T>& P = d.sims[s];
-        const T* r = rec_cur(d, ldcg(d.clock + s)) + (size_t)g * RECW;
+        const T* r = rec_cur(d, par) + (size_t)g * RECW;
         int cx, cy;
         grid_coords(P, ldcg(r + R_X), ldcg(r + R_Y), cx, cy);
         const int cell = P.cell_off + cx + P.ncx * cy;
@@ -207,12 +246,12 @@ __device__ void phase_sort(const DevPtrs<T>& d, int tid, int nthr) {
 // reference's order (oy outer, ox inner), candidates in perm order, kept if
 // |ri - rj| <= rmax_i + rmax_j + range (exactly rounded like the oracle).
 template <class T>
-__device__ void phase_neighbors(const DevPtrs<T>& d, int tid, int nthr) {
+__device__ void phase_neighbors(const DevPtrs<T>& d, int par, int tid, int nthr) {
     for (int g = tid; g < d.Ntot; g += nthr) {
         const int s = __ldg(d.sim_of + g);
         if (!(ldcg(d.flags + s) & F_NEED)) continue;
         const SimDesc<T>& P = d.sims[s];
-        const T* rc = rec_cur(d, ldcg(d.clock + s));
+        const T* rc = rec_cur(d, par);
         const T xi = ldcg(rc + (size_t)g * RECW + R_X), yi = ldcg(rc + (size_t)g * RECW + R_Y);
         const T rmi = ldcg(rc + (size_t)g * RECW + R_RMAX);
         const T ri = add_rn(rmi, P.nbrange);
@@ -321,8 +360,8 @@ __device__ __forceinline__ void substrate_displacement(const DevPtrs<T>& d, cons
 // are the group-reduced gradients (uniform across the group).
 template <class T, int L>
 __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T>& P, bool act, int g, int s, int l,
-                                            long long clk, const T (&rv)[RECW], T r0, int ti, T fx, T fy, T tt,
-                                            const T (&gl)[NCM], const UpdatePre<T, L>& pre, bool split) {
+                                            int par, long long clk, const T (&rv)[RECW], T r0, int ti, T fx, T fy,
+                                            T tt, const T (&gl)[NCM], const UpdatePre<T, L>& pre, bool split) {
     constexpr unsigned FULL = 0xffffffffu;
     constexpr int MPL = UpdatePre<T, L>::MPL;
     const T dt = P.dt;
@@ -340,6 +379,7 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
     T* cf = d.coef + (size_t)(act ? g : 0) * NCM;
     const T a0 = pre.a0;
     const T ga0 = r0 * gl[0];
+    const T h0 = ga0 / (T(2) * a0);  // dE/da0 * da0/da_n = -h0 a_n (area constraint)
     const T dtmu = dt * P.muab[ti];
     const int K = P.K;
     T an[MPL], bn[MPL];
@@ -359,8 +399,8 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
             T so, co;
             t_sincos(T(m + 2) * tho, &so, &co);
             const T a = pre.a[u], b = pre.b[u];
-            const T gca = ga * co + gb * so - ga0 * a / (T(2) * a0);
-            const T gcb = -ga * so + gb * co - ga0 * b / (T(2) * a0);
+            const T gca = ga * co + gb * so - h0 * a;
+            const T gcb = -ga * so + gb * co - h0 * b;
             an[u] = a - dtmu * gca;
             bn[u] = b - dtmu * gcb;
             sp += sqrt((double)an[u] * (double)an[u] + (double)bn[u] * (double)bn[u]);
@@ -383,7 +423,7 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
     const T a0n = T(sqrt(1.0 - qs * 0.5));
 
     // lab frame of the new state (src/geometry.jl:208-227)
-    T* rn = rec_next(d, clk) + (size_t)(act ? g : 0) * RECW;
+    T* rn = rec_next(d, par) + (size_t)(act ? g : 0) * RECW;
     T bp = T(0);
 #pragma unroll
     for (int u = 0; u < MPL; ++u) {
@@ -407,7 +447,7 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
     if (act && l == 0) {
         T dxp, dyp;
         if (split) {
-            const T* rc = rec_cur(d, clk);
+            const T* rc = rec_cur(d, par);
             if (P.parent_drag[ti]) {
                 const int c = unpack_w(rv[R_W]) >> 3;
                 T ux, uy;
@@ -456,6 +496,16 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
     }
 }
 
+// A simulation that does not step (frozen or an empty slot) keeps its state:
+// its records are copied into the next buffer.
+template <class T, int L>
+__device__ __forceinline__ void carry_record(const DevPtrs<T>& d, int g, int l, int par, const T (&rv)[RECW]) {
+    T* rn = rec_next(d, par) + (size_t)g * RECW;
+#pragma unroll
+    for (int u = 0; u < RECW; ++u)
+        if ((u & (L - 1)) == l) rn[u] = rv[u];
+}
+
 // ==================================================== force evaluation ==
 enum : int { MODE_FUSED = 0, MODE_FORCES = 1, MODE_DIAG = 2 };
 
@@ -469,27 +519,28 @@ enum : int { MODE_FUSED = 0, MODE_FORCES = 1, MODE_DIAG = 2 };
 //   bond forces                                 src/energies/bonds.jl:98-111
 //   pullback glab = S' Gall                     src/gradients.jl:374-386
 template <class T, int L, int S, bool ONE, int MODE>
-__device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stage) {
+__device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stage, int par) {
     constexpr int BPW = 32 / L;
     constexpr unsigned FULL = 0xffffffffu;
     constexpr int CH16 = RECW * (int)sizeof(T) / 16;  // 16-byte chunks per record
     const int lane = threadIdx.x & 31;
     const int l = lane & (L - 1);
     const int g = wg * BPW + lane / L;
-    bool act = g < d.Ntot;
-    const int s = act ? __ldg(d.sim_of + g) : 0;
-    const int fl = ldcg(d.flags + s);
-    if (MODE != MODE_DIAG) act = act && (fl & F_ACTIVE) && !(fl & F_FROZEN);
-    const int gg = act ? g : 0;
-    const SimDesc<T>& P = d.sims[s];
-    const long long clk = ldcg(d.clock + s);
-    const T* rc = rec_cur(d, clk);
-    const int nth = P.nth;
-    const T dphi = P.dphi;
-
-    // ---- early loads: own record, neighbour list, staged neighbour records, update operands
+    const bool valid = g < d.Ntot;
+    const int gg = valid ? g : 0;
+    const T* rc = rec_cur(d, par);
+    // ---- early loads: own record, simulation state, neighbour list, staged
+    // neighbour records, update operands
     T rv[RECW];
     load_rec(rc + (size_t)gg * RECW, rv);
+    const int s = __ldg(d.sim_of + gg);
+    const int fl = ldcg(d.flags + s);
+    const long long clk = ldcg(d.clock + s);
+    bool act = valid;
+    if (MODE != MODE_DIAG) act = act && (fl & F_ACTIVE) && !(fl & F_FROZEN);
+    const SimDesc<T>& P = d.sims[s];
+    const int nth = P.nth;
+    const T dphi = P.dphi;
     const T r0 = __ldg(d.R0 + gg);
     const bool contact = act && (fl & F_CONTACT);
     const int cnt = contact ? min(ldcg(d.nb_count + gg), d.cap) : 0;
@@ -556,7 +607,11 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
         synth(ch);
 #pragma unroll
         for (int sl = 0; sl < S; ++sl)
-            if (vmask & (1u << sl)) Qp += t_sqrt(R[sl] * R[sl] + R1[sl] * R1[sl]);
+            if (vmask & (1u << sl)) {
+                T q, iq;
+                norm_inv(R[sl] * R[sl] + R1[sl] * R1[sl], q, iq);
+                Qp += q;
+            }
     }
     const T Q = group_sum<L>(Qp) * dphi;
 
@@ -614,7 +669,8 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                 for (int qq = 0; qq < qn; ++qq) {
                     const bool qa = base + qq < cnt;
                     const T* nrec = snb + qq * RECW;
-                    const T xj = nrec[R_X], yj = nrec[R_Y], rmj = nrec[R_RMAX], wj = nrec[R_W];
+                    T xj, yj, rmj, wj;
+                    lds_head(nrec, xj, yj, rmj, wj);
                     const T dxc = minimum_image_fast(xi - xj, Lx, iLx);
                     const T dyc = minimum_image_fast(yi - yj, Ly, iLy);
                     const T lim = rmj + crange;
@@ -631,6 +687,13 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                             if ((vmask & (1u << sl)) && dx * dx + dy * dy <= lim2) hm |= 1u << sl;
                         }
                     }
+                    // pair coupling of the terms (src/energies/contact.jl:267-293)
+                    T gA = T(0), gB = T(0);
+                    if (hm) {
+                        const int wjv = unpack_w(wj);
+                        gA = P.cA[(wjv >> 3) == pi ? 1 : 0][ti][wjv & 7];
+                        gB = P.cB[ti];
+                    }
                     // one hit per lane per round: the hit path runs as many rounds as
                     // the busiest lane has hits for this neighbour (usually one)
                     while (__any_sync(FULL, hm != 0)) {
@@ -646,28 +709,28 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                                 dx = minimum_image_fast(dx, Lx, iLx);
                                 dy = minimum_image_fast(dy, Ly, iLy);
                             }
-                            const T dist = t_sqrt(dx * dx + dy * dy);
-                            T cp = T(1), sp = T(0);
-                            if (dist > T(0)) {
-                                const T inv = T(1) / dist;
+                            const T d2 = dx * dx + dy * dy;
+                            T dist = T(0), cp = T(1), sp = T(0);
+                            if (d2 > T(0)) {  // direction of u - r_j (psi = 0 at u = r_j, like atan(0, 0))
+                                T inv;
+                                norm_inv(d2, dist, inv);
                                 cp = dx * inv;
                                 sp = dy * inv;
                             }
+                            T lj[20];
+                            lds_lab(nrec, lj);
                             // R_j(psi) by the angle-addition recurrence (src/geometry.jl:282-291)
-                            T c = cp, sn = sp, rj = nrec[R_A0];
+                            T c = cp, sn = sp, rj = lj[0];
 #pragma unroll
                             for (int m = 0; m < KM; ++m) {
                                 const T cn = c * cp - sn * sp;
                                 sn = sn * cp + c * sp;
                                 c = cn;
-                                rj += nrec[R_AL + m] * c + nrec[R_BE + m] * sn;
+                                rj += lj[1 + m] * c + lj[1 + KM + m] * sn;
                             }
                             const T dd = rj - dist;
-                            const int wjv = unpack_w(wj);
-                            const int tj = wjv & 7;
-                            const int rel = (wjv >> 3) == pi ? 1 : 0;
-                            T gv = dd >= T(0) ? P.cA[rel][ti][tj] : T(0);
-                            if (dd > T(0)) gv += P.cB[ti] * dd;
+                            T gv = dd >= T(0) ? gA : T(0);
+                            if (dd > T(0)) gv += gB * dd;
 #pragma unroll
                             for (int u = 0; u < S; ++u)
                                 if (sl == u) p[u] += gv;
@@ -681,8 +744,8 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
         for (int sl = 0; sl < S; ++sl) {
             if (!(vmask & (1u << sl))) continue;
             const T r = R[sl], r1 = R1[sl], c1 = C1[sl], s1 = S1[sl];
-            const T q = t_sqrt(r * r + r1 * r1);
-            const T iq = T(1) / q;
+            T q, iq;
+            norm_inv(r * r + r1 * r1, q, iq);
             const T pw = p[sl] * dphi;
             const T GRk = W * r * iq + pw * r;
             const T GDk = W * r1 * iq;
@@ -762,6 +825,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
             const T* cf = d.coef + (size_t)g * NCM;
             const T a0 = ldcg(cf);
             const T ga0 = r0 * gl[0];
+            const T h0 = ga0 / (T(2) * a0);
             const T tho = rv[R_TH];
 #pragma unroll
             for (int u = 0; u < (KM + L - 1) / L; ++u) {
@@ -776,8 +840,8 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                 T so, co;
                 t_sincos(T(m + 2) * tho, &so, &co);
                 const T a = ldcg(cf + 1 + m), b = ldcg(cf + 1 + KM + m);
-                d.gcoef[(size_t)g * NCM + 1 + m] = ga * co + gb * so - ga0 * a / (T(2) * a0);
-                d.gcoef[(size_t)g * NCM + 1 + KM + m] = -ga * so + gb * co - ga0 * b / (T(2) * a0);
+                d.gcoef[(size_t)g * NCM + 1 + m] = ga * co + gb * so - h0 * a;
+                d.gcoef[(size_t)g * NCM + 1 + KM + m] = -ga * so + gb * co - h0 * b;
             }
             if (l == 0) d.gcoef[(size_t)g * NCM] = ga0;
         }
@@ -792,26 +856,28 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
         d.gth[g] = tt;
         d.E[g] = E;
     }
-    update_body<T, L>(d, P, act, g, s, l, clk, rv, r0, ti, fx, fy, tt, gl, pre, false);
+    if (valid && !act) carry_record<T, L>(d, g, l, par, rv);
+    update_body<T, L>(d, P, act, g, s, l, par, clk, rv, r0, ti, fx, fy, tt, gl, pre, false);
 }
 
 // Phase B of the split step: displacement with parent drag + update of the
 // bodies of warp group `wg`, from the forces phase A stored.
 template <class T, int L>
-__device__ __forceinline__ void update_warp_split(const DevPtrs<T>& d, int wg) {
+__device__ __forceinline__ void update_warp_split(const DevPtrs<T>& d, int wg, int par) {
     constexpr int BPW = 32 / L;
     const int lane = threadIdx.x & 31;
     const int l = lane & (L - 1);
     const int g = wg * BPW + lane / L;
-    bool act = g < d.Ntot;
-    const int s = act ? __ldg(d.sim_of + g) : 0;
+    const bool valid = g < d.Ntot;
+    const int gg = valid ? g : 0;
+    const int s = __ldg(d.sim_of + gg);
     const int fl = ldcg(d.flags + s);
-    act = act && (fl & F_ACTIVE) && !(fl & F_FROZEN);
-    const int gg = act ? g : 0;
+    const bool act = valid && (fl & F_ACTIVE) && !(fl & F_FROZEN);
     const SimDesc<T>& P = d.sims[s];
     const long long clk = ldcg(d.clock + s);
     T rv[RECW];
-    load_rec(rec_cur(d, clk) + (size_t)gg * RECW, rv);
+    load_rec(rec_cur(d, par) + (size_t)gg * RECW, rv);
+    if (valid && !act) carry_record<T, L>(d, g, l, par, rv);
     const int ti = unpack_w(rv[R_W]) & 7;
     const T r0 = __ldg(d.R0 + gg);
     UpdatePre<T, L> pre;
@@ -820,7 +886,7 @@ __device__ __forceinline__ void update_warp_split(const DevPtrs<T>& d, int wg) {
 #pragma unroll
     for (int r = 0; r < NCM; ++r) gl[r] = ldcg(d.glab + (size_t)gg * NCM + r);
     const T fx = ldcg(d.gx + gg), fy = ldcg(d.gy + gg), tt = ldcg(d.gth + gg);
-    update_body<T, L>(d, P, act, g, s, l, clk, rv, r0, ti, fx, fy, tt, gl, pre, true);
+    update_body<T, L>(d, P, act, g, s, l, par, clk, rv, r0, ti, fx, fy, tt, gl, pre, true);
 }
 
 // Last block of a step's closing barrier: tick the clocks of the simulations
@@ -852,9 +918,9 @@ __device__ void bookkeeping(const DevPtrs<T>& d) {
 
 // ============================================================= kernels ==
 template <class T>
-__device__ __forceinline__ bool rebuild_prologue(const DevPtrs<T>& d, int tid, int nthr) {
+__device__ __forceinline__ bool rebuild_prologue(const DevPtrs<T>& d, int par, int tid, int nthr) {
     auto noop = [] {};
-    phase_count(d, tid, nthr);
+    phase_count(d, par, tid, nthr);
     if (!grid_barrier(d.sync, noop)) return false;
     phase_scan(d);
     if (!grid_barrier(d.sync, noop)) return false;
@@ -862,7 +928,7 @@ __device__ __forceinline__ bool rebuild_prologue(const DevPtrs<T>& d, int tid, i
     if (!grid_barrier(d.sync, noop)) return false;
     phase_sort(d, tid, nthr);
     if (!grid_barrier(d.sync, noop)) return false;
-    phase_neighbors(d, tid, nthr);
+    phase_neighbors(d, par, tid, nthr);
     return grid_barrier(d.sync, noop);
 }
 
@@ -875,8 +941,8 @@ __device__ __forceinline__ T* warp_stage(size_t bytes_per_warp) {
 
 // Persistent cooperative step kernel: `nsteps` whole time steps per launch.
 // Each block takes a contiguous range of warp groups (balanced bodies per SM).
-template <class T, int L, int S, bool ONE, bool SPLIT, int BLK>
-__global__ void __launch_bounds__(BLK) k_step(DevPtrs<T> d, int nsteps) {
+template <class T, int L, int S, bool ONE, bool SPLIT, int BLK, int MINB>
+__global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, int par0) {
     constexpr int WPB = BLK / 32;
     const int warp = threadIdx.x >> 5;
     const int ngroups = (d.Ntot + (32 / L) - 1) / (32 / L);
@@ -886,13 +952,14 @@ __global__ void __launch_bounds__(BLK) k_step(DevPtrs<T> d, int nsteps) {
     const int nthr = gridDim.x * blockDim.x;
     T* stage = warp_stage<T>(stage_bytes_per_warp<T, L>());
     for (int st = 0; st < nsteps; ++st) {
+        const int par = (par0 + st) & 1;
         if (ld_acquire(&d.sync->any_need))
-            if (!rebuild_prologue(d, tid, nthr)) return;
+            if (!rebuild_prologue(d, par, tid, nthr)) return;
         for (int wg = g0 + warp; wg < g1; wg += WPB)
-            forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage);
+            forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage, par);
         if (SPLIT) {
             if (!grid_barrier(d.sync, [] {})) return;
-            for (int wg = g0 + warp; wg < g1; wg += WPB) update_warp_split<T, L>(d, wg);
+            for (int wg = g0 + warp; wg < g1; wg += WPB) update_warp_split<T, L>(d, wg, par);
         }
         if (!grid_barrier(d.sync, [&] { bookkeeping(d); })) return;
     }
@@ -901,19 +968,19 @@ __global__ void __launch_bounds__(BLK) k_step(DevPtrs<T> d, int nsteps) {
 // compute_gradients! (src/simulation.jl:150-158): forces and every gradient
 // buffer of the current state, no update.
 template <class T, int L, int S, bool ONE>
-__global__ void __launch_bounds__(256) k_gradients(DevPtrs<T> d) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_gradients(DevPtrs<T> d, int par) {
     const int wpb = blockDim.x >> 5;
     const int wg = blockIdx.x * wpb + (threadIdx.x >> 5);
     const int ngroups = (d.Ntot + (32 / L) - 1) / (32 / L);
     T* stage = warp_stage<T>(stage_bytes_per_warp<T, L>());
-    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG>(d, wg, stage);
+    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG>(d, wg, stage, par);
 }
 
 // Stand-alone rebuild phases (update_neighbors!, and the stateless neighbour
 // build), one launch per phase.
 template <class T>
-__global__ void k_phase_count(DevPtrs<T> d) {
-    if (ldcg(&d.sync->any_need)) phase_count(d, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+__global__ void k_phase_count(DevPtrs<T> d, int par) {
+    if (ldcg(&d.sync->any_need)) phase_count(d, par, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 template <class T>
 __global__ void k_phase_scan(DevPtrs<T> d) {
@@ -928,13 +995,13 @@ __global__ void k_phase_sort(DevPtrs<T> d) {
     if (ldcg(&d.sync->any_need)) phase_sort(d, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 template <class T>
-__global__ void k_phase_neighbors(DevPtrs<T> d) {
-    if (ldcg(&d.sync->any_need)) phase_neighbors(d, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+__global__ void k_phase_neighbors(DevPtrs<T> d, int par) {
+    if (ldcg(&d.sync->any_need)) phase_neighbors(d, par, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // Skin check of the current state (skin_check_kernel!, src/neighbors.jl:188-194).
 template <class T>
-__global__ void k_skin_check(DevPtrs<T> d) {
+__global__ void k_skin_check(DevPtrs<T> d, int par) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= d.Ntot) return;
     const int s = __ldg(d.sim_of + g);
@@ -942,7 +1009,7 @@ __global__ void k_skin_check(DevPtrs<T> d) {
     if (!(f & F_CONTACT) || !(f & F_VALID)) return;
     const SimDesc<T>& P = d.sims[s];
     if (!(P.skin > T(0))) return;
-    const T* r = rec_cur(d, ldcg(d.clock + s)) + (size_t)g * RECW;
+    const T* r = rec_cur(d, par) + (size_t)g * RECW;
     const T dx = minimum_image_exact(sub_rn(ldcg(r + R_X), ldcg(d.x0 + g)), P.Lx);
     const T dy = minimum_image_exact(sub_rn(ldcg(r + R_Y), ldcg(d.y0 + g)), P.Ly);
     const T grow = sub_rn(ldcg(r + R_RMAX), ldcg(d.rmax0 + g));
@@ -990,11 +1057,11 @@ __global__ void k_finish_rebuild(DevPtrs<T> d) {
 }
 
 // Simulation set-up and set_state: enforce_shape! (FP64 sums) and the lab
-// frame of the given body state into rec[clock & 1] (src/simulation.jl:102-103,
+// frame of the given body state into rec[par] (src/simulation.jl:102-103,
 // src/dynamics.jl:44-64, src/geometry.jl:208-227).  One thread per body.
 template <class T>
-__global__ void k_init(DevPtrs<T> d, const T* __restrict__ x, const T* __restrict__ y, const T* __restrict__ th,
-                       const T* __restrict__ coef_in) {
+__global__ void k_init(DevPtrs<T> d, int par, const T* __restrict__ x, const T* __restrict__ y,
+                       const T* __restrict__ th, const T* __restrict__ coef_in) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= d.Ntot) return;
     const int s = d.sim_of[g];
@@ -1016,8 +1083,8 @@ __global__ void k_init(DevPtrs<T> d, const T* __restrict__ x, const T* __restric
     for (int m = 0; m < K; ++m) q += (double)c[1 + m] * c[1 + m] + (double)c[1 + KM + m] * c[1 + KM + m];
     c[0] = T(sqrt(1.0 - q * 0.5));
     const T r0 = d.R0[g];
-    T* rn = rec_cur_mut(d, d.clock[s]) + (size_t)g * RECW;
-    T* ro = rec_next(d, d.clock[s]) + (size_t)g * RECW;
+    T* rn = rec_cur_mut(d, par) + (size_t)g * RECW;
+    T* ro = rec_next(d, par) + (size_t)g * RECW;
     T bound = c[0];
     for (int r = 0; r < RECW; ++r) ro[r] = T(0);
     for (int m = 0; m < KM; ++m) {
@@ -1043,23 +1110,23 @@ __global__ void k_init(DevPtrs<T> d, const T* __restrict__ x, const T* __restric
 
 // w field (parent, type) of the current record
 template <class T>
-__global__ void k_set_w(DevPtrs<T> d, const int* __restrict__ w) {
+__global__ void k_set_w(DevPtrs<T> d, int par, const int* __restrict__ w) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= d.Ntot) return;
     T* tag = nullptr;
-    rec_cur_mut(d, d.clock[d.sim_of[g]])[(size_t)g * RECW + R_W] = pack_w(w[g], tag);
+    rec_cur_mut(d, par)[(size_t)g * RECW + R_W] = pack_w(w[g], tag);
 }
 
 // Geometry of the current state for get_geometry: lab, labR0, rmax, and
 // R, R', R'' at the nodes (src/geometry.jl:13-32, 248-257).  Outputs in the
 // engine's fixed coefficient layout [a0; a_2..a_10; b_2..b_10].
 template <class T>
-__global__ void k_geometry(DevPtrs<T> d, T* lab, T* labR0, T* R, T* dR, T* ddR, T* rmax) {
+__global__ void k_geometry(DevPtrs<T> d, int par, T* lab, T* labR0, T* R, T* dR, T* ddR, T* rmax) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= d.Ntot) return;
     const int s = d.sim_of[g];
     const SimDesc<T>& P = d.sims[s];
-    const T* rc = rec_cur(d, d.clock[s]) + (size_t)g * RECW;
+    const T* rc = rec_cur(d, par) + (size_t)g * RECW;
     const T* cf = d.coef + (size_t)g * NCM;
     const T r0 = d.R0[g];
     const T th = rc[R_TH];
@@ -1101,12 +1168,12 @@ __global__ void k_geometry(DevPtrs<T> d, T* lab, T* labR0, T* R, T* dR, T* ddR, 
 
 // perimeters, areas, shape index with FP64 node sums (src/observables.jl:7-18).
 template <class T>
-__global__ void k_observables(DevPtrs<T> d, double* out) {
+__global__ void k_observables(DevPtrs<T> d, int par, double* out) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= d.Ntot) return;
     const int s = d.sim_of[g];
     const SimDesc<T>& P = d.sims[s];
-    const T* rc = rec_cur(d, d.clock[s]) + (size_t)g * RECW;
+    const T* rc = rec_cur(d, par) + (size_t)g * RECW;
     double per = 0.0, area = 0.0;
     for (int k = 0; k < P.nth; ++k) {
         const T c1 = d.cs[2 * k], s1 = d.cs[2 * k + 1];

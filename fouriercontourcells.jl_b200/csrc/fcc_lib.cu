@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -78,9 +79,34 @@ struct DBuf {
 
 const double PI = 3.14159265358979323846;
 
-// Launch configuration of the force/update kernels for nθ (lanes per body,
-// node slots per lane); see fcc_kernels.cuh.
-constexpr int LANES = 8, SLOTS = 5, BLOCK = 256;
+// Launch configurations of the step kernel: lanes per body L, node slots per
+// lane S (L*S >= 40 covers the nθ = 40 contour in one pass), and the minimum
+// resident 256-thread blocks per SM the register budget is cut for.
+constexpr int BLOCK = 256;
+
+template <class T, int L, int S, int MB>
+void* step_fn(bool one, bool split) {
+    if (one)
+        return split ? (void*)k_step<T, L, S, true, true, BLOCK, MB> : (void*)k_step<T, L, S, true, false, BLOCK, MB>;
+    return split ? (void*)k_step<T, L, S, false, true, BLOCK, MB> : (void*)k_step<T, L, S, false, false, BLOCK, MB>;
+}
+
+struct Variant {
+    int L, S, minb;
+    void* (*f32)(bool, bool);
+    void* (*f64)(bool, bool);
+    size_t stage32, stage64;  // shared-memory neighbour stage per warp
+};
+
+const Variant VARIANTS[] = {
+    {8, 5, 2, step_fn<float, 8, 5, 2>, step_fn<double, 8, 5, 1>, stage_bytes_per_warp<float, 8>(), stage_bytes_per_warp<double, 8>()},
+    {4, 10, 2, step_fn<float, 4, 10, 2>, nullptr, stage_bytes_per_warp<float, 4>(), 0},
+    {16, 3, 2, step_fn<float, 16, 3, 2>, nullptr, stage_bytes_per_warp<float, 16>(), 0},
+    {8, 5, 3, step_fn<float, 8, 5, 3>, nullptr, stage_bytes_per_warp<float, 8>(), 0},
+    {4, 10, 1, step_fn<float, 4, 10, 1>, nullptr, stage_bytes_per_warp<float, 4>(), 0},
+};
+constexpr int NVARIANTS = sizeof(VARIANTS) / sizeof(VARIANTS[0]);
+constexpr int LANES = 8, SLOTS = 5;  // compute_gradients and the FP64 step
 
 struct EngineBase {
     virtual ~EngineBase() = default;
@@ -114,6 +140,7 @@ struct Engine final : EngineBase {
     std::vector<T> R0_h;
     // host mirror of run state
     long long clock_h = 0;
+    long long gstep = 0;  // engine step counter: the current record buffer is rec[gstep & 1]
     T t_h = T(0);
     int64_t step_h = 0;
     int64_t builds_adjust = 0;
@@ -457,29 +484,38 @@ struct Engine final : EngineBase {
         return sync_stream();
     }
 
-    static constexpr size_t stage_bytes() { return (size_t)(BLOCK / 32) * stage_bytes_per_warp<T, LANES>(); }
-
-    // the persistent step kernel variant for this simulation
-    void* step_kernel() const {
-        if (one_chunk())
-            return split ? (void*)k_step<T, LANES, SLOTS, true, true, BLOCK> : (void*)k_step<T, LANES, SLOTS, true, false, BLOCK>;
-        return split ? (void*)k_step<T, LANES, SLOTS, false, true, BLOCK> : (void*)k_step<T, LANES, SLOTS, false, false, BLOCK>;
-    }
+    int variant = 0;
+    const Variant& var() const { return VARIANTS[variant]; }
+    static constexpr size_t grad_stage_bytes() { return (size_t)(256 / 32) * stage_bytes_per_warp<T, LANES>(); }
+    size_t stage_bytes() const { return (size_t)(BLOCK / 32) * (sizeof(T) == 4 ? var().stage32 : var().stage64); }
+    void* step_kernel() const { return (sizeof(T) == 4 ? var().f32 : var().f64)(one_chunk(), split); }
     void* grad_kernel() const {
-        return one_chunk() ? (void*)k_gradients<T, LANES, SLOTS, true> : (void*)k_gradients<T, LANES, SLOTS, false>;
+        return nth <= LANES * SLOTS ? (void*)k_gradients<T, LANES, SLOTS, true> : (void*)k_gradients<T, LANES, SLOTS, false>;
     }
 
-    bool one_chunk() const { return nth <= LANES * SLOTS; }
+    bool one_chunk() const { return nth <= var().L * var().S; }
+
+    // Variant choice: FCC_VARIANT overrides; FP64 always uses variant 0.
+    void choose_variant() {
+        variant = 0;
+        if (sizeof(T) != 4) return;
+        if (const char* e = std::getenv("FCC_VARIANT")) {
+            const int v = std::atoi(e);
+            if (v >= 0 && v < NVARIANTS) variant = v;
+        }
+    }
 
     fcc_status configure() {
+        choose_variant();
         const int smem = (int)stage_bytes();
-        for (void* fn : {step_kernel(), grad_kernel()})
-            CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        CUDA_TRY(cudaFuncSetAttribute(step_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        CUDA_TRY(cudaFuncSetAttribute(grad_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_stage_bytes()));
         int per_sm = 0;
         CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_kernel(), BLOCK, smem));
         if (per_sm < 1) return fail(FCC_ERR_UNSUPPORTED, "step kernel does not fit on an SM");
         const int maxblocks = per_sm * nsm;
-        const int64_t groups = (N + (32 / LANES) - 1) / (32 / LANES);
+        const int bpw = 32 / var().L;
+        const int64_t groups = (N + bpw - 1) / bpw;
         const int64_t want = std::max<int64_t>(1, (groups + BLOCK / 32 - 1) / (BLOCK / 32));
         step_grid = (int)std::min<int64_t>(want, maxblocks);
         return FCC_OK;
@@ -518,9 +554,9 @@ struct Engine final : EngineBase {
         const DevPtrs<T> d = ptrs();
         if (N > 0) {
             const int grid = (int)((N + 255) / 256);
-            k_init<T><<<grid, 256, 0, stream>>>(d, bx.p, by.p, bth.p, bc.p);
+            k_init<T><<<grid, 256, 0, stream>>>(d, par(), bx.p, by.p, bth.p, bc.p);
             CUDA_TRY(cudaGetLastError());
-            k_set_w<T><<<grid, 256, 0, stream>>>(d, bw.p);
+            k_set_w<T><<<grid, 256, 0, stream>>>(d, par(), bw.p);
             CUDA_TRY(cudaGetLastError());
         }
         // list invalid: the next step (or update_neighbors!) rebuilds
@@ -530,6 +566,8 @@ struct Engine final : EngineBase {
         CUDA_TRY(cudaMemcpyAsync(sync.p, &gs, sizeof(GridSync), cudaMemcpyHostToDevice, stream));
         return sync_stream();  // staging buffers are freed on return
     }
+
+    int par() const { return (int)(gstep & 1); }
 
     fcc_status sync_stream() {
         CUDA_TRY(cudaStreamSynchronize(stream));
@@ -571,8 +609,10 @@ struct Engine final : EngineBase {
 
     fcc_status launch_steps(int nsteps) {
         DevPtrs<T> d = ptrs();
-        void* args[] = {&d, &nsteps};
+        int p0 = par();
+        void* args[] = {&d, &nsteps, &p0};
         CUDA_TRY(cudaLaunchCooperativeKernel(step_kernel(), dim3(step_grid), dim3(BLOCK), args, stage_bytes(), stream));
+        gstep += nsteps;
         ++last_launches;
         return FCC_OK;
     }
@@ -643,15 +683,15 @@ struct Engine final : EngineBase {
         for (int attempt = 0; attempt < 8; ++attempt) {
             DevPtrs<T> dd = ptrs();
             if (!force && attempt == 0) {
-                k_skin_check<T><<<grid, 256, 0, stream>>>(dd);
+                k_skin_check<T><<<grid, 256, 0, stream>>>(dd, par());
                 CUDA_TRY(cudaGetLastError());
             }
             k_prepare_rebuild<T><<<1, 256, 0, stream>>>(dd, (force || attempt > 0) ? 1 : 0);
-            k_phase_count<T><<<grid, 256, 0, stream>>>(dd);
+            k_phase_count<T><<<grid, 256, 0, stream>>>(dd, par());
             k_phase_scan<T><<<1, 1024, 0, stream>>>(dd);
             k_phase_scatter<T><<<grid, 256, 0, stream>>>(dd);
             k_phase_sort<T><<<(ncx * ncy + 255) / 256, 256, 0, stream>>>(dd);
-            k_phase_neighbors<T><<<grid, 256, 0, stream>>>(dd);
+            k_phase_neighbors<T><<<grid, 256, 0, stream>>>(dd, par());
             k_finish_rebuild<T><<<1, 256, 0, stream>>>(dd);
             CUDA_TRY(cudaGetLastError());
             FCC_TRY(read_status());
@@ -679,10 +719,10 @@ struct Engine final : EngineBase {
         const DevPtrs<T> d = ptrs();
         const int64_t groups = (N + (32 / LANES) - 1) / (32 / LANES);
         const int grid = (int)((groups + 256 / 32 - 1) / (256 / 32));
-        if (one_chunk())
-            k_gradients<T, LANES, SLOTS, true><<<grid, 256, stage_bytes(), stream>>>(d);
+        if (nth <= LANES * SLOTS)
+            k_gradients<T, LANES, SLOTS, true><<<grid, 256, grad_stage_bytes(), stream>>>(d, par());
         else
-            k_gradients<T, LANES, SLOTS, false><<<grid, 256, stage_bytes(), stream>>>(d);
+            k_gradients<T, LANES, SLOTS, false><<<grid, 256, grad_stage_bytes(), stream>>>(d, par());
         CUDA_TRY(cudaGetLastError());
         return sync_stream();
     }
@@ -710,7 +750,7 @@ struct Engine final : EngineBase {
             if (o->n != N || o->ncoef != nc) return fail(FCC_ERR_DIMENSION, "state buffers do not match the simulation");
             std::vector<T> rec, cf;
             std::vector<int> ix, iy;
-            FCC_TRY(fetch((clock_h & 1) ? rec1.p : rec0.p, (size_t)N * RECW, rec));
+            FCC_TRY(fetch(par() ? rec1.p : rec0.p, (size_t)N * RECW, rec));
             FCC_TRY(fetch(coef.p, (size_t)N * NCM, cf));
             FCC_TRY(fetch(imgx.p, (size_t)N, ix));
             FCC_TRY(fetch(imgy.p, (size_t)N, iy));
@@ -795,7 +835,7 @@ struct Engine final : EngineBase {
         FCC_TRY(dR.alloc(n * nth, stream));
         FCC_TRY(ddR.alloc(n * nth, stream));
         FCC_TRY(rmax.alloc(n, stream));
-        k_geometry<T><<<(int)((N + 127) / 128), 128, 0, stream>>>(ptrs(), lab.p, labR0.p, R.p, dR.p, ddR.p, rmax.p);
+        k_geometry<T><<<(int)((N + 127) / 128), 128, 0, stream>>>(ptrs(), par(), lab.p, labR0.p, R.p, dR.p, ddR.p, rmax.p);
         CUDA_TRY(cudaGetLastError());
         std::vector<T> a;
         auto nodes = [&](DBuf<T>& src, double* dst) -> fcc_status {
@@ -877,7 +917,7 @@ struct Engine final : EngineBase {
         if (N > 0) {
             DBuf<double> buf;
             FCC_TRY(buf.alloc(3 * (size_t)N, stream));
-            k_observables<T><<<(int)((N + 127) / 128), 128, 0, stream>>>(ptrs(), buf.p);
+            k_observables<T><<<(int)((N + 127) / 128), 128, 0, stream>>>(ptrs(), par(), buf.p);
             CUDA_TRY(cudaGetLastError());
             CUDA_TRY(cudaMemcpyAsync(v.data(), buf.p, v.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
             FCC_TRY(sync_stream());
@@ -994,11 +1034,11 @@ fcc_status build_neighbors_t(int64_t n, const double* x, const double* y, const 
     d.sync = sync.p;
     const int grid = (int)((N + 255) / 256);
     k_pack_head<T><<<grid, 256, 0, st>>>(rec.p, xd.p, yd.p, rd.p, (int)N);
-    k_phase_count<T><<<grid, 256, 0, st>>>(d);
+    k_phase_count<T><<<grid, 256, 0, st>>>(d, 0);
     k_phase_scan<T><<<1, 1024, 0, st>>>(d);
     k_phase_scatter<T><<<grid, 256, 0, st>>>(d);
     k_phase_sort<T><<<(int)((C + 255) / 256), 256, 0, st>>>(d);
-    k_phase_neighbors<T><<<grid, 256, 0, st>>>(d);
+    k_phase_neighbors<T><<<grid, 256, 0, st>>>(d, 0);
     CUDA_TRY(cudaGetLastError());
     std::vector<int> a, b, cnt;
     a.resize(N);
@@ -1141,7 +1181,7 @@ fcc_status fcc_build_neighbors(int32_t precision, int64_t n, const double* x, co
 const char* fcc_last_error(void) { return g_err.c_str(); }
 
 const char* fcc_version(void) {
-    return "libfcc_b200 sm_100a: persistent cooperative step kernel, 8 lanes x 5 nodes per body";
+    return "libfcc_b200 sm_100a: persistent cooperative step kernel (lanes x nodes per body: 8x5, 4x10, 16x3)";
 }
 
 }  // extern "C"
