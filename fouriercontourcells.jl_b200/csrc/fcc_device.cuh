@@ -59,7 +59,7 @@ struct SimDesc {
     int ncx, ncy, cell_off, ncells;
     int body_off, n, nth, K;
     uint32_t k0, k1;  // Philox key
-    int ntypes, rewrap, has_contact, has_parent_drag;
+    int ntypes, rewrap, has_contact, has_parent_drag, has_noise;
     int nbt, nbd;
     T v0[MT], Dr[MT], Dt[MT], mur[MT], muth[MT], muab[MT];
     int parent_drag[MT];

@@ -327,6 +327,26 @@ __device__ __forceinline__ void load_update_pre(const DevPtrs<T>& d, int gg, int
     }
 }
 
+// (cos n t, sin n t) from (cos t, sin t) by binary powering, n = 2..10 (a
+// few complex products instead of one sincos per mode).
+template <class T>
+__device__ __forceinline__ void cis_pow(T c1, T s1, int n, T& cn, T& sn) {
+    T rc = T(1), rs = T(0), bc = c1, bs = s1;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        if (n & (1 << b)) {
+            const T t = rc * bc - rs * bs;
+            rs = rc * bs + rs * bc;
+            rc = t;
+        }
+        const T t = bc * bc - bs * bs;
+        bs = T(2) * bc * bs;
+        bc = t;
+    }
+    cn = rc;
+    sn = rs;
+}
+
 // Translational displacement of a body with substrate drag, plus the forces
 // of its children with parent drag (src/dynamics.jl:84-99).
 template <class T>
@@ -361,20 +381,23 @@ __device__ __forceinline__ void substrate_displacement(const DevPtrs<T>& d, cons
 template <class T, int L>
 __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T>& P, bool act, int g, int s, int l,
                                             int par, long long clk, const T (&rv)[RECW], T r0, int ti, T fx, T fy,
-                                            T tt, const T (&gl)[NCM], const UpdatePre<T, L>& pre, bool split) {
+                                            T tt, const T (&gl)[NCM], const UpdatePre<T, L>& pre, int fl,
+                                            const T (&nz)[2], bool split) {
     constexpr unsigned FULL = 0xffffffffu;
     constexpr int MPL = UpdatePre<T, L>::MPL;
     const T dt = P.dt;
     const T tho = rv[R_TH];
     const uint32_t li = (uint32_t)(g - P.body_off + 1);
+    // standard normals of this body and step (src/random.jl:88-100): lane 0
+    // holds block 1 (orientation), lane 1 block 0 (translation)
+    const T z3 = __shfl_sync(FULL, nz[0], 0, L);
+    const T xi1 = __shfl_sync(FULL, nz[0], 1, L);
+    const T xi2 = __shfl_sync(FULL, nz[1], 1, L);
     const T sig_r = t_sqrt(T(2) * P.Dr[ti] * dt);
-    T z3 = T(0);
-    if (act && l == 0 && sig_r != T(0)) {
-        T z4;
-        philox_pair<T>(P.k0, P.k1, li, (uint64_t)clk, 1u, z3, z4);
-    }
-    z3 = __shfl_sync(FULL, z3, 0, L);
     const T thn = tho - (dt * P.muth[ti]) * tt + sig_r * z3;
+    T so1, co1, sn1, cn1;
+    t_sincos(tho, &so1, &co1);
+    t_sincos(thn, &sn1, &cn1);
 
     T* cf = d.coef + (size_t)(act ? g : 0) * NCM;
     const T a0 = pre.a0;
@@ -397,13 +420,13 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
             ga *= r0;
             gb *= r0;
             T so, co;
-            t_sincos(T(m + 2) * tho, &so, &co);
+            cis_pow(co1, so1, m + 2, co, so);
             const T a = pre.a[u], b = pre.b[u];
             const T gca = ga * co + gb * so - h0 * a;
             const T gcb = -ga * so + gb * co - h0 * b;
             an[u] = a - dtmu * gca;
             bn[u] = b - dtmu * gcb;
-            sp += sqrt((double)an[u] * (double)an[u] + (double)bn[u] * (double)bn[u]);
+            sp += (double)t_sqrt(an[u] * an[u] + bn[u] * bn[u]);
         }
     }
     // enforce_shape! (src/dynamics.jl:44-64) with FP64 sums
@@ -430,7 +453,7 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
         const int m = l + u * L;
         if (m < K) {
             T so, co;
-            t_sincos(T(m + 2) * thn, &so, &co);
+            cis_pow(cn1, sn1, m + 2, co, so);
             const T al = an[u] * co - bn[u] * so;
             const T be = an[u] * so + bn[u] * co;
             bp += t_sqrt(an[u] * an[u] + bn[u] * bn[u]);
@@ -452,24 +475,16 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
                 const int c = unpack_w(rv[R_W]) >> 3;
                 T ux, uy;
                 substrate_displacement(d, P, rc, c, clk, ux, uy);
-                T so, co;
-                t_sincos(tho, &so, &co);
                 const T sig = t_sqrt(T(2) * P.Dt[ti] * dt);
-                T x1 = T(0), x2 = T(0);
-                if (sig != T(0)) philox_pair<T>(P.k0, P.k1, li, (uint64_t)clk, 0u, x1, x2);
-                dxp = ux + dt * (P.v0[ti] * co - P.mur[ti] * fx) + sig * x1;
-                dyp = uy + dt * (P.v0[ti] * so - P.mur[ti] * fy) + sig * x2;
+                dxp = ux + dt * (P.v0[ti] * co1 - P.mur[ti] * fx) + sig * xi1;
+                dyp = uy + dt * (P.v0[ti] * so1 - P.mur[ti] * fy) + sig * xi2;
             } else {
                 substrate_displacement(d, P, rc, g, clk, dxp, dyp);
             }
         } else {
-            T so, co;
-            t_sincos(tho, &so, &co);
             const T sig = t_sqrt(T(2) * P.Dt[ti] * dt);
-            T x1 = T(0), x2 = T(0);
-            if (sig != T(0)) philox_pair<T>(P.k0, P.k1, li, (uint64_t)clk, 0u, x1, x2);
-            dxp = dt * (P.v0[ti] * co - P.mur[ti] * fx) + sig * x1;
-            dyp = dt * (P.v0[ti] * so - P.mur[ti] * fy) + sig * x2;
+            dxp = dt * (P.v0[ti] * co1 - P.mur[ti] * fx) + sig * xi1;
+            dyp = dt * (P.v0[ti] * so1 - P.mur[ti] * fy) + sig * xi2;
         }
         int sx, sy;
         const T xw = wrap_exact(add_rn(rv[R_X], dxp), P.Lx, sx);
@@ -483,9 +498,9 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
         rn[R_A0] = r0 * a0n;
         rn[R_TH] = thn;
         cf[0] = a0n;
-        const int f = ldcg(d.flags + s);
-        // skin check of the new state (src/neighbors.jl:198-205)
-        if ((f & F_CONTACT) && (f & F_VALID) && P.skin > T(0)) {
+        // skin check of the new state (src/neighbors.jl:198-205); the flags of
+        // this step (read at its start) already carry F_VALID of a rebuild
+        if ((fl & F_CONTACT) && (fl & F_VALID) && P.skin > T(0)) {
             const T dx = minimum_image_exact(sub_rn(xw, pre.x0), P.Lx);
             const T dy = minimum_image_exact(sub_rn(yw, pre.y0), P.Ly);
             const T grow = sub_rn(rmax, pre.rmax0);
@@ -519,41 +534,59 @@ enum : int { MODE_FUSED = 0, MODE_FORCES = 1, MODE_DIAG = 2 };
 //   bond forces                                 src/energies/bonds.jl:98-111
 //   pullback glab = S' Gall                     src/gradients.jl:374-386
 template <class T, int L, int S, bool ONE, int MODE>
-__device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stage, int par) {
+__device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stage, int par, const SimDesc<T>* sim0) {
     constexpr int BPW = 32 / L;
     constexpr unsigned FULL = 0xffffffffu;
     constexpr int CH16 = RECW * (int)sizeof(T) / 16;  // 16-byte chunks per record
+    constexpr int IDS = (NBMAX + L - 1) / L;           // staged neighbour ids per lane
     const int lane = threadIdx.x & 31;
     const int l = lane & (L - 1);
     const int g = wg * BPW + lane / L;
     const bool valid = g < d.Ntot;
     const int gg = valid ? g : 0;
     const T* rc = rec_cur(d, par);
-    // ---- early loads: own record, simulation state, neighbour list, staged
-    // neighbour records, update operands
+    // ---- independent loads first: own record, neighbour count and ids,
+    // simulation state, update operands
     T rv[RECW];
     load_rec(rc + (size_t)gg * RECW, rv);
-    const int s = __ldg(d.sim_of + gg);
+    const int s = sim0 ? 0 : __ldg(d.sim_of + gg);
+    const SimDesc<T>& P = sim0 ? *sim0 : d.sims[s];
+    const T r0 = __ldg(d.R0 + gg);
+    const int cnt_raw = ldcg(d.nb_count + gg);
+    int ids[IDS];
+#pragma unroll
+    for (int u = 0; u < IDS; ++u) {
+        const int q = l + u * L;
+        ids[u] = q < min(d.cap, NBMAX) ? ldcg(d.nb_idx + (size_t)gg * d.cap + q) : gg;
+    }
     const int fl = ldcg(d.flags + s);
     const long long clk = ldcg(d.clock + s);
+    UpdatePre<T, L> pre;
+    if (MODE == MODE_FUSED) load_update_pre(d, gg, l, P.K, pre);
     bool act = valid;
     if (MODE != MODE_DIAG) act = act && (fl & F_ACTIVE) && !(fl & F_FROZEN);
-    const SimDesc<T>& P = d.sims[s];
     const int nth = P.nth;
     const T dphi = P.dphi;
-    const T r0 = __ldg(d.R0 + gg);
+
+    // ---- Philox normals of this body and step, early so their latency hides
+    // behind the loads: lane 1 draws block 0 (translation), the other lanes
+    // block 1 (orientation) (src/random.jl:75-100)
+    T nz[2] = {T(0), T(0)};
+    if (MODE == MODE_FUSED && P.has_noise)
+        philox_pair<T>(P.k0, P.k1, (uint32_t)(gg - P.body_off + 1), (uint64_t)clk, l == 1 ? 0u : 1u, nz[0], nz[1]);
+
+    // ---- stage the neighbour records in shared memory (cp.async)
     const bool contact = act && (fl & F_CONTACT);
-    const int cnt = contact ? min(ldcg(d.nb_count + gg), d.cap) : 0;
+    const int cnt = contact ? min(cnt_raw, d.cap) : 0;
     T* snb = stage + (size_t)(lane / L) * NBMAX * RECW;
-    // stage the records of neighbours [base, base + NBMAX) of this body
     auto stage_batch = [&](int base) {
         const int npre = min(cnt - base, NBMAX);
         __syncwarp();  // every lane is done with the previous contents
 #pragma unroll
-        for (int u = 0; u < (NBMAX + L - 1) / L; ++u) {
+        for (int u = 0; u < IDS; ++u) {
             const int q = l + u * L;
             if (q < npre) {
-                const int j = ldcg(d.nb_idx + (size_t)gg * d.cap + base + q);
+                const int j = base == 0 ? ids[u] : ldcg(d.nb_idx + (size_t)gg * d.cap + base + q);
                 const T* src = rc + (size_t)j * RECW;
 #pragma unroll
                 for (int c = 0; c < CH16; ++c) cp_async16(snb + q * RECW + c * (16 / sizeof(T)), src + c * (16 / sizeof(T)));
@@ -563,8 +596,6 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
     };
     stage_batch(0);
     int staged_base = 0;
-    UpdatePre<T, L> pre;
-    if (MODE == MODE_FUSED) load_update_pre(d, gg, l, P.K, pre);
 
     const int wv = unpack_w(rv[R_W]);
     const int ti = wv & 7;
@@ -857,27 +888,30 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
         d.E[g] = E;
     }
     if (valid && !act) carry_record<T, L>(d, g, l, par, rv);
-    update_body<T, L>(d, P, act, g, s, l, par, clk, rv, r0, ti, fx, fy, tt, gl, pre, false);
+    update_body<T, L>(d, P, act, g, s, l, par, clk, rv, r0, ti, fx, fy, tt, gl, pre, fl, nz, false);
 }
 
 // Phase B of the split step: displacement with parent drag + update of the
 // bodies of warp group `wg`, from the forces phase A stored.
 template <class T, int L>
-__device__ __forceinline__ void update_warp_split(const DevPtrs<T>& d, int wg, int par) {
+__device__ __forceinline__ void update_warp_split(const DevPtrs<T>& d, int wg, int par, const SimDesc<T>* sim0) {
     constexpr int BPW = 32 / L;
     const int lane = threadIdx.x & 31;
     const int l = lane & (L - 1);
     const int g = wg * BPW + lane / L;
     const bool valid = g < d.Ntot;
     const int gg = valid ? g : 0;
-    const int s = __ldg(d.sim_of + gg);
+    const int s = sim0 ? 0 : __ldg(d.sim_of + gg);
     const int fl = ldcg(d.flags + s);
     const bool act = valid && (fl & F_ACTIVE) && !(fl & F_FROZEN);
-    const SimDesc<T>& P = d.sims[s];
+    const SimDesc<T>& P = sim0 ? *sim0 : d.sims[s];
     const long long clk = ldcg(d.clock + s);
     T rv[RECW];
     load_rec(rec_cur(d, par) + (size_t)gg * RECW, rv);
     if (valid && !act) carry_record<T, L>(d, g, l, par, rv);
+    T nz[2] = {T(0), T(0)};
+    if (P.has_noise)
+        philox_pair<T>(P.k0, P.k1, (uint32_t)(gg - P.body_off + 1), (uint64_t)clk, l == 1 ? 0u : 1u, nz[0], nz[1]);
     const int ti = unpack_w(rv[R_W]) & 7;
     const T r0 = __ldg(d.R0 + gg);
     UpdatePre<T, L> pre;
@@ -886,7 +920,7 @@ __device__ __forceinline__ void update_warp_split(const DevPtrs<T>& d, int wg, i
 #pragma unroll
     for (int r = 0; r < NCM; ++r) gl[r] = ldcg(d.glab + (size_t)gg * NCM + r);
     const T fx = ldcg(d.gx + gg), fy = ldcg(d.gy + gg), tt = ldcg(d.gth + gg);
-    update_body<T, L>(d, P, act, g, s, l, par, clk, rv, r0, ti, fx, fy, tt, gl, pre, true);
+    update_body<T, L>(d, P, act, g, s, l, par, clk, rv, r0, ti, fx, fy, tt, gl, pre, fl, nz, true);
 }
 
 // Last block of a step's closing barrier: tick the clocks of the simulations
@@ -932,6 +966,18 @@ __device__ __forceinline__ bool rebuild_prologue(const DevPtrs<T>& d, int par, i
     return grid_barrier(d.sync, noop);
 }
 
+// A single simulation's descriptor is read from shared memory (copied once per
+// block); an engine holding several reads each body's from global memory.
+template <class T>
+__device__ __forceinline__ const SimDesc<T>* copy_desc(const DevPtrs<T>& d) {
+    __shared__ __align__(16) unsigned s_desc[(sizeof(SimDesc<T>) + 3) / 4];
+    if (d.nsims != 1) return nullptr;
+    const unsigned* src = reinterpret_cast<const unsigned*>(d.sims);
+    for (int u = threadIdx.x; u < (int)((sizeof(SimDesc<T>) + 3) / 4); u += blockDim.x) s_desc[u] = src[u];
+    __syncthreads();
+    return reinterpret_cast<const SimDesc<T>*>(s_desc);
+}
+
 // Dynamic shared memory of the force kernels: one neighbour stage per warp.
 template <class T>
 __device__ __forceinline__ T* warp_stage(size_t bytes_per_warp) {
@@ -951,15 +997,16 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nthr = gridDim.x * blockDim.x;
     T* stage = warp_stage<T>(stage_bytes_per_warp<T, L>());
+    const SimDesc<T>* sim0 = copy_desc(d);
     for (int st = 0; st < nsteps; ++st) {
         const int par = (par0 + st) & 1;
         if (ld_acquire(&d.sync->any_need))
             if (!rebuild_prologue(d, par, tid, nthr)) return;
         for (int wg = g0 + warp; wg < g1; wg += WPB)
-            forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage, par);
+            forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage, par, sim0);
         if (SPLIT) {
             if (!grid_barrier(d.sync, [] {})) return;
-            for (int wg = g0 + warp; wg < g1; wg += WPB) update_warp_split<T, L>(d, wg, par);
+            for (int wg = g0 + warp; wg < g1; wg += WPB) update_warp_split<T, L>(d, wg, par, sim0);
         }
         if (!grid_barrier(d.sync, [&] { bookkeeping(d); })) return;
     }
@@ -973,7 +1020,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_gradients(DevPt
     const int wg = blockIdx.x * wpb + (threadIdx.x >> 5);
     const int ngroups = (d.Ntot + (32 / L) - 1) / (32 / L);
     T* stage = warp_stage<T>(stage_bytes_per_warp<T, L>());
-    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG>(d, wg, stage, par);
+    const SimDesc<T>* sim0 = copy_desc(d);
+    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG>(d, wg, stage, par, sim0);
 }
 
 // Stand-alone rebuild phases (update_neighbors!, and the stateless neighbour

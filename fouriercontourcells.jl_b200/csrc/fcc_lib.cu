@@ -388,6 +388,9 @@ struct Engine final : EngineBase {
             }
         }
         s.has_contact = has_contact ? 1 : 0;
+        s.has_noise = 0;
+        for (int t = 0; t < p->ntypes; ++t)
+            if (p->types[t].Dr != 0 || p->types[t].Dt != 0) s.has_noise = 1;
         split = false;
         for (int64_t i = 0; i < N; ++i)
             if (p->types[b->type[i] - 1].parent_drag) split = true;
