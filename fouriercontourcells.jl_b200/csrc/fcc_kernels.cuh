@@ -689,6 +689,8 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                 rcx[sl] = R[sl] * C1[sl];
                 rcy[sl] = R[sl] * S1[sl];
             }
+            // neighbours in batches of the stage (one batch unless a list is long)
+            constexpr int QB = 64 / S;  // neighbours per 64-bit hit mask
             for (int base = 0; base < maxc; base += NBMAX) {
                 if (base != staged_base) {  // lists longer than the stage: restage
                     stage_batch(base);
@@ -697,75 +699,79 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                     staged_base = base;
                 }
                 const int qn = min(maxc - base, NBMAX);
-                for (int qq = 0; qq < qn; ++qq) {
-                    const bool qa = base + qq < cnt;
-                    const T* nrec = snb + qq * RECW;
-                    T xj, yj, rmj, wj;
-                    lds_head(nrec, xj, yj, rmj, wj);
-                    const T dxc = minimum_image_fast(xi - xj, Lx, iLx);
-                    const T dyc = minimum_image_fast(yi - yj, Ly, iLy);
-                    const T lim = rmj + crange;
-                    const T lim2 = lim * lim;
-                    unsigned hm = 0;
-                    if (qa) {
+                for (int q0 = 0; q0 < qn; q0 += QB) {
+                    // (1) bounding-circle test of every node against every staged
+                    // neighbour: bit (q - q0) * S + slot of a 64-bit hit mask
+                    unsigned long long hm = 0;
+                    const int q1 = min(qn, q0 + QB);
+                    for (int qq = q0; qq < q1; ++qq) {
+                        if (base + qq < cnt) {
+                            T xj, yj, rmj, wj;
+                            lds_head(snb + qq * RECW, xj, yj, rmj, wj);
+                            const T dxc = minimum_image_fast(xi - xj, Lx, iLx);
+                            const T dyc = minimum_image_fast(yi - yj, Ly, iLy);
+                            const T lim = rmj + crange;
+                            const T lim2 = lim * lim;
 #pragma unroll
-                        for (int sl = 0; sl < S; ++sl) {
-                            T dx = rcx[sl] + dxc, dy = rcy[sl] + dyc;
-                            if (rewrap) {
-                                dx = minimum_image_fast(dx, Lx, iLx);
-                                dy = minimum_image_fast(dy, Ly, iLy);
+                            for (int sl = 0; sl < S; ++sl) {
+                                T dx = rcx[sl] + dxc, dy = rcy[sl] + dyc;
+                                if (rewrap) {
+                                    dx = minimum_image_fast(dx, Lx, iLx);
+                                    dy = minimum_image_fast(dy, Ly, iLy);
+                                }
+                                if ((vmask & (1u << sl)) && dx * dx + dy * dy <= lim2)
+                                    hm |= 1ull << ((qq - q0) * S + sl);
                             }
-                            if ((vmask & (1u << sl)) && dx * dx + dy * dy <= lim2) hm |= 1u << sl;
                         }
                     }
-                    // pair coupling of the terms (src/energies/contact.jl:267-293)
-                    T gA = T(0), gB = T(0);
-                    if (hm) {
+                    // (2) every lane walks its own hits in (neighbour, node) order, so
+                    // each node sums its neighbours' g(d) in list order
+                    // (src/energies/contact.jl:309-322)
+                    while (hm) {
+                        const int bit = __ffsll((long long)hm) - 1;
+                        hm &= hm - 1;
+                        const int qq = q0 + bit / S;
+                        const int sl = bit - (bit / S) * S;
+                        const T* nrec = snb + qq * RECW;
+                        T xj, yj, rmj, wj;
+                        lds_head(nrec, xj, yj, rmj, wj);
+                        T rx = rcx[0], ry = rcy[0];
+#pragma unroll
+                        for (int u = 1; u < S; ++u)
+                            if (sl == u) rx = rcx[u], ry = rcy[u];
+                        T dx = rx + minimum_image_fast(xi - xj, Lx, iLx);
+                        T dy = ry + minimum_image_fast(yi - yj, Ly, iLy);
+                        if (rewrap) {
+                            dx = minimum_image_fast(dx, Lx, iLx);
+                            dy = minimum_image_fast(dy, Ly, iLy);
+                        }
+                        const T d2 = dx * dx + dy * dy;
+                        T dist = T(0), cp = T(1), sp = T(0);
+                        if (d2 > T(0)) {  // direction of u - r_j (psi = 0 at u = r_j, like atan(0, 0))
+                            T inv;
+                            norm_inv(d2, dist, inv);
+                            cp = dx * inv;
+                            sp = dy * inv;
+                        }
+                        T lj[20];
+                        lds_lab(nrec, lj);
+                        // R_j(psi) by the angle-addition recurrence (src/geometry.jl:282-291)
+                        T c = cp, sn = sp, rj = lj[0];
+#pragma unroll
+                        for (int m = 0; m < KM; ++m) {
+                            const T cn = c * cp - sn * sp;
+                            sn = sn * cp + c * sp;
+                            c = cn;
+                            rj += lj[1 + m] * c + lj[1 + KM + m] * sn;
+                        }
+                        const T dd = rj - dist;
+                        // pair coupling of the terms (src/energies/contact.jl:267-293)
                         const int wjv = unpack_w(wj);
-                        gA = P.cA[(wjv >> 3) == pi ? 1 : 0][ti][wjv & 7];
-                        gB = P.cB[ti];
-                    }
-                    // one hit per lane per round: the hit path runs as many rounds as
-                    // the busiest lane has hits for this neighbour (usually one)
-                    while (__any_sync(FULL, hm != 0)) {
-                        if (hm) {
-                            const int sl = __ffs(hm) - 1;
-                            hm &= hm - 1;
-                            T rx = rcx[0], ry = rcy[0];
+                        T gv = dd >= T(0) ? P.cA[(wjv >> 3) == pi ? 1 : 0][ti][wjv & 7] : T(0);
+                        if (dd > T(0)) gv += P.cB[ti] * dd;
 #pragma unroll
-                            for (int u = 1; u < S; ++u)
-                                if (sl == u) rx = rcx[u], ry = rcy[u];
-                            T dx = rx + dxc, dy = ry + dyc;
-                            if (rewrap) {
-                                dx = minimum_image_fast(dx, Lx, iLx);
-                                dy = minimum_image_fast(dy, Ly, iLy);
-                            }
-                            const T d2 = dx * dx + dy * dy;
-                            T dist = T(0), cp = T(1), sp = T(0);
-                            if (d2 > T(0)) {  // direction of u - r_j (psi = 0 at u = r_j, like atan(0, 0))
-                                T inv;
-                                norm_inv(d2, dist, inv);
-                                cp = dx * inv;
-                                sp = dy * inv;
-                            }
-                            T lj[20];
-                            lds_lab(nrec, lj);
-                            // R_j(psi) by the angle-addition recurrence (src/geometry.jl:282-291)
-                            T c = cp, sn = sp, rj = lj[0];
-#pragma unroll
-                            for (int m = 0; m < KM; ++m) {
-                                const T cn = c * cp - sn * sp;
-                                sn = sn * cp + c * sp;
-                                c = cn;
-                                rj += lj[1 + m] * c + lj[1 + KM + m] * sn;
-                            }
-                            const T dd = rj - dist;
-                            T gv = dd >= T(0) ? gA : T(0);
-                            if (dd > T(0)) gv += gB * dd;
-#pragma unroll
-                            for (int u = 0; u < S; ++u)
-                                if (sl == u) p[u] += gv;
-                        }
+                        for (int u = 0; u < S; ++u)
+                            if (sl == u) p[u] += gv;
                     }
                 }
             }
