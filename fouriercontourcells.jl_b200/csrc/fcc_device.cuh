@@ -7,7 +7,8 @@
 //                  step counter (current = rec[par]).  Neighbours read it,
 //                  so a step reads rec[par] and writes rec[par^1]:
 //                    [0] x  [1] y  [2] rmax  [3] w = parent_global<<3 | (type-1)
-//                    [4] R0*a0  [5..13] R0*alpha_n  [14..22] R0*beta_n  [23] theta
+//                    [4] R0*a0  [5 + 2m] R0*alpha_n  [6 + 2m] R0*beta_n  [23] theta
+//                    (n = m + 2; alpha/beta interleaved so a mode is one 8-byte pair)
 //                  (lab-frame coefficients scaled by R0, src/geometry.jl:208-227;
 //                  modes n = 2..10 at fixed slots, unused modes stay zero).
 //                  96 B (FP32) per body = six 16-byte vector loads.
@@ -36,7 +37,9 @@ constexpr int MTERM = 16;    // max terms
 constexpr double SHAPE_BOUND = 0.816496580927726;  // sqrt(2/3), src/dynamics.jl:26
 
 // record slots
-constexpr int R_X = 0, R_Y = 1, R_RMAX = 2, R_W = 3, R_A0 = 4, R_AL = 5, R_BE = 14, R_TH = 23;
+constexpr int R_X = 0, R_Y = 1, R_RMAX = 2, R_W = 3, R_A0 = 4, R_TH = 23;
+__host__ __device__ constexpr int r_al(int m) { return 5 + 2 * m; }  // R0*alpha of mode n = m + 2
+__host__ __device__ constexpr int r_be(int m) { return 6 + 2 * m; }  // R0*beta of mode n = m + 2
 
 // per-simulation flags
 enum : int {

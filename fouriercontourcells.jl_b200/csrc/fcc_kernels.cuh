@@ -115,6 +115,61 @@ __device__ __forceinline__ void lds_lab(const double* p, double (&c)[20]) {
     for (int u = 0; u < 20; ++u) c[u] = p[R_A0 + u];
 }
 
+// R_j(psi) = R0 [a0 + sum_n alpha_n cos n psi + beta_n sin n psi] of a staged
+// record at direction (cp, sp) = (cos psi, sin psi), by angle addition
+// (src/geometry.jl:282-291) run as two independent chains, even and odd n,
+// both stepping by 2 psi.  Coefficients are loaded as they are consumed.
+__device__ __forceinline__ float radius_at(const float* p, float cp, float sp) {
+    const float c2 = cp * cp - sp * sp, s2 = 2.f * cp * sp;  // 2 psi
+    const float c3 = c2 * cp - s2 * sp, s3 = s2 * cp + c2 * sp;  // 3 psi
+    float4 v = lds4(p + R_A0);  // a0, al2, be2, al3
+    float re = v.y * c2 + v.z * s2;
+    float ro = v.w * c3;
+    float ce = c2, se = s2, co = c3, so = s3;
+    const float a0 = v.x;
+    v = lds4(p + R_A0 + 4);  // be3, al4, be4, al5
+    ro += v.x * s3;
+    float t = ce * c2 - se * s2;
+    se = se * c2 + ce * s2, ce = t;  // 4 psi
+    re += v.y * ce + v.z * se;
+    t = co * c2 - so * s2;
+    so = so * c2 + co * s2, co = t;  // 5 psi
+    ro += v.w * co;
+    v = lds4(p + R_A0 + 8);  // be5, al6, be6, al7
+    ro += v.x * so;
+    t = ce * c2 - se * s2;
+    se = se * c2 + ce * s2, ce = t;  // 6 psi
+    re += v.y * ce + v.z * se;
+    t = co * c2 - so * s2;
+    so = so * c2 + co * s2, co = t;  // 7 psi
+    ro += v.w * co;
+    v = lds4(p + R_A0 + 12);  // be7, al8, be8, al9
+    ro += v.x * so;
+    t = ce * c2 - se * s2;
+    se = se * c2 + ce * s2, ce = t;  // 8 psi
+    re += v.y * ce + v.z * se;
+    t = co * c2 - so * s2;
+    so = so * c2 + co * s2, co = t;  // 9 psi
+    ro += v.w * co;
+    v = lds4(p + R_A0 + 16);  // be9, al10, be10, theta
+    ro += v.x * so;
+    t = ce * c2 - se * s2;
+    se = se * c2 + ce * s2, ce = t;  // 10 psi
+    re += v.y * ce + v.z * se;
+    return a0 + (re + ro);
+}
+__device__ __forceinline__ double radius_at(const double* p, double cp, double sp) {
+    double c = cp, sn = sp, r = p[R_A0];
+#pragma unroll
+    for (int m = 0; m < KM; ++m) {
+        const double cn = c * cp - sn * sp;
+        sn = sn * cp + c * sp;
+        c = cn;
+        r += p[r_al(m)] * c + p[r_be(m)] * sn;
+    }
+    return r;
+}
+
 // |u| and 1/|u| of a contour node distance (FP32: one rsqrt)
 __device__ __forceinline__ void norm_inv(float x2, float& n, float& inv) {
     inv = rsqrtf(x2);
@@ -458,8 +513,8 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
             const T be = an[u] * so + bn[u] * co;
             bp += t_sqrt(an[u] * an[u] + bn[u] * bn[u]);
             if (act) {
-                rn[R_AL + m] = r0 * al;
-                rn[R_BE + m] = r0 * be;
+                rn[r_al(m)] = r0 * al;
+                rn[r_be(m)] = r0 * be;
                 cf[1 + m] = an[u];
                 cf[1 + KM + m] = bn[u];
             }
@@ -622,7 +677,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                 const T cn = c * c1 - sn * s1;
                 sn = sn * c1 + c * s1;
                 c = cn;
-                const T al = rv[R_AL + m], be = rv[R_BE + m];
+                const T al = rv[r_al(m)], be = rv[r_be(m)];
                 r += al * c + be * sn;
                 r1 += n * (be * c - al * sn);
             }
@@ -666,9 +721,11 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
 
     // ---- pass 2: contact pressure, contour gradients, force/torque and pullback partials
     T fx = T(0), fy = T(0), tt = T(0);
-    T gl[NCM];
+    T gl[NCM];  // pullback accumulators: live only from the gradient section on (one chunk)
+    if (!ONE) {
 #pragma unroll
-    for (int r = 0; r < NCM; ++r) gl[r] = T(0);
+        for (int r = 0; r < NCM; ++r) gl[r] = T(0);
+    }
 
     cp_async_wait_all();
     __syncwarp();
@@ -683,12 +740,6 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
 #pragma unroll
         for (int sl = 0; sl < S; ++sl) p[sl] = T(0);
         if (maxc > 0) {
-            T rcx[S], rcy[S];
-#pragma unroll
-            for (int sl = 0; sl < S; ++sl) {
-                rcx[sl] = R[sl] * C1[sl];
-                rcy[sl] = R[sl] * S1[sl];
-            }
             // neighbours in batches of the stage (one batch unless a list is long)
             constexpr int QB = 64 / S;  // neighbours per 64-bit hit mask
             for (int base = 0; base < maxc; base += NBMAX) {
@@ -714,7 +765,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                             const T lim2 = lim * lim;
 #pragma unroll
                             for (int sl = 0; sl < S; ++sl) {
-                                T dx = rcx[sl] + dxc, dy = rcy[sl] + dyc;
+                                T dx = R[sl] * C1[sl] + dxc, dy = R[sl] * S1[sl] + dyc;
                                 if (rewrap) {
                                     dx = minimum_image_fast(dx, Lx, iLx);
                                     dy = minimum_image_fast(dy, Ly, iLy);
@@ -735,12 +786,12 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                         const T* nrec = snb + qq * RECW;
                         T xj, yj, rmj, wj;
                         lds_head(nrec, xj, yj, rmj, wj);
-                        T rx = rcx[0], ry = rcy[0];
+                        T rr = R[0], rcs = C1[0], rsn = S1[0];
 #pragma unroll
                         for (int u = 1; u < S; ++u)
-                            if (sl == u) rx = rcx[u], ry = rcy[u];
-                        T dx = rx + minimum_image_fast(xi - xj, Lx, iLx);
-                        T dy = ry + minimum_image_fast(yi - yj, Ly, iLy);
+                            if (sl == u) rr = R[u], rcs = C1[u], rsn = S1[u];
+                        T dx = rr * rcs + minimum_image_fast(xi - xj, Lx, iLx);
+                        T dy = rr * rsn + minimum_image_fast(yi - yj, Ly, iLy);
                         if (rewrap) {
                             dx = minimum_image_fast(dx, Lx, iLx);
                             dy = minimum_image_fast(dy, Ly, iLy);
@@ -753,18 +804,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                             cp = dx * inv;
                             sp = dy * inv;
                         }
-                        T lj[20];
-                        lds_lab(nrec, lj);
-                        // R_j(psi) by the angle-addition recurrence (src/geometry.jl:282-291)
-                        T c = cp, sn = sp, rj = lj[0];
-#pragma unroll
-                        for (int m = 0; m < KM; ++m) {
-                            const T cn = c * cp - sn * sp;
-                            sn = sn * cp + c * sp;
-                            c = cn;
-                            rj += lj[1 + m] * c + lj[1 + KM + m] * sn;
-                        }
-                        const T dd = rj - dist;
+                        const T dd = radius_at(nrec, cp, sp) - dist;
                         // pair coupling of the terms (src/energies/contact.jl:267-293)
                         const int wjv = unpack_w(wj);
                         T gv = dd >= T(0) ? P.cA[(wjv >> 3) == pi ? 1 : 0][ti][wjv & 7] : T(0);
@@ -775,6 +815,10 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                     }
                 }
             }
+        }
+        if (ONE) {
+#pragma unroll
+            for (int r = 0; r < NCM; ++r) gl[r] = T(0);
         }
         // contour gradients of node k: GR = W R/q + p dphi R, GD = W R'/q, GDD = 0
 #pragma unroll
@@ -1150,8 +1194,8 @@ __global__ void k_init(DevPtrs<T> d, int par, const T* __restrict__ x, const T* 
             be = c[1 + m] * so + c[1 + KM + m] * co;
             bound += t_sqrt(c[1 + m] * c[1 + m] + c[1 + KM + m] * c[1 + KM + m]);
         }
-        rn[R_AL + m] = r0 * al;
-        rn[R_BE + m] = r0 * be;
+        rn[r_al(m)] = r0 * al;
+        rn[r_be(m)] = r0 * be;
     }
     rn[R_X] = x[g];
     rn[R_Y] = y[g];
@@ -1196,8 +1240,8 @@ __global__ void k_geometry(DevPtrs<T> d, int par, T* lab, T* labR0, T* R, T* dR,
         }
         lab[(size_t)g * NCM + 1 + m] = al;
         lab[(size_t)g * NCM + 1 + KM + m] = be;
-        labR0[(size_t)g * NCM + 1 + m] = rc[R_AL + m];
-        labR0[(size_t)g * NCM + 1 + KM + m] = rc[R_BE + m];
+        labR0[(size_t)g * NCM + 1 + m] = rc[r_al(m)];
+        labR0[(size_t)g * NCM + 1 + KM + m] = rc[r_be(m)];
     }
     rmax[g] = rc[R_RMAX];
     for (int k = 0; k < P.nth; ++k) {
@@ -1208,7 +1252,7 @@ __global__ void k_geometry(DevPtrs<T> d, int par, T* lab, T* labR0, T* R, T* dR,
             const T cn = c * c1 - sn * s1;
             sn = sn * c1 + c * s1;
             c = cn;
-            const T al = rc[R_AL + m], be = rc[R_BE + m];
+            const T al = rc[r_al(m)], be = rc[r_be(m)];
             const T t = al * c + be * sn;
             r += t;
             r1 += n * (be * c - al * sn);
@@ -1237,7 +1281,7 @@ __global__ void k_observables(DevPtrs<T> d, int par, double* out) {
             const T cn = c * c1 - sn * s1;
             sn = sn * c1 + c * s1;
             c = cn;
-            const T al = rc[R_AL + m], be = rc[R_BE + m];
+            const T al = rc[r_al(m)], be = rc[r_be(m)];
             r += al * c + be * sn;
             r1 += n * (be * c - al * sn);
         }

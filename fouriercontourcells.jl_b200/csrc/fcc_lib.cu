@@ -84,26 +84,27 @@ const double PI = 3.14159265358979323846;
 // resident 256-thread blocks per SM the register budget is cut for.
 constexpr int BLOCK = 256;
 
-template <class T, int L, int S, int MB>
+template <class T, int L, int S, int BLK, int MB>
 void* step_fn(bool one, bool split) {
     if (one)
-        return split ? (void*)k_step<T, L, S, true, true, BLOCK, MB> : (void*)k_step<T, L, S, true, false, BLOCK, MB>;
-    return split ? (void*)k_step<T, L, S, false, true, BLOCK, MB> : (void*)k_step<T, L, S, false, false, BLOCK, MB>;
+        return split ? (void*)k_step<T, L, S, true, true, BLK, MB> : (void*)k_step<T, L, S, true, false, BLK, MB>;
+    return split ? (void*)k_step<T, L, S, false, true, BLK, MB> : (void*)k_step<T, L, S, false, false, BLK, MB>;
 }
 
 struct Variant {
-    int L, S, minb;
+    int L, S, blk, minb;
     void* (*f32)(bool, bool);
     void* (*f64)(bool, bool);
     size_t stage32, stage64;  // shared-memory neighbour stage per warp
 };
 
 const Variant VARIANTS[] = {
-    {8, 5, 2, step_fn<float, 8, 5, 2>, step_fn<double, 8, 5, 1>, stage_bytes_per_warp<float, 8>(), stage_bytes_per_warp<double, 8>()},
-    {4, 10, 2, step_fn<float, 4, 10, 2>, nullptr, stage_bytes_per_warp<float, 4>(), 0},
-    {16, 3, 2, step_fn<float, 16, 3, 2>, nullptr, stage_bytes_per_warp<float, 16>(), 0},
-    {8, 5, 3, step_fn<float, 8, 5, 3>, nullptr, stage_bytes_per_warp<float, 8>(), 0},
-    {4, 10, 1, step_fn<float, 4, 10, 1>, nullptr, stage_bytes_per_warp<float, 4>(), 0},
+    {8, 5, 256, 2, step_fn<float, 8, 5, 256, 2>, step_fn<double, 8, 5, 256, 1>, stage_bytes_per_warp<float, 8>(),
+     stage_bytes_per_warp<double, 8>()},
+    {4, 10, 256, 2, step_fn<float, 4, 10, 256, 2>, nullptr, stage_bytes_per_warp<float, 4>(), 0},
+    {16, 3, 256, 2, step_fn<float, 16, 3, 256, 2>, nullptr, stage_bytes_per_warp<float, 16>(), 0},
+    {8, 5, 128, 5, step_fn<float, 8, 5, 128, 5>, nullptr, stage_bytes_per_warp<float, 8>(), 0},
+    {16, 3, 128, 5, step_fn<float, 16, 3, 128, 5>, nullptr, stage_bytes_per_warp<float, 16>(), 0},
 };
 constexpr int NVARIANTS = sizeof(VARIANTS) / sizeof(VARIANTS[0]);
 constexpr int LANES = 8, SLOTS = 5;  // compute_gradients and the FP64 step
@@ -490,7 +491,7 @@ struct Engine final : EngineBase {
     int variant = 0;
     const Variant& var() const { return VARIANTS[variant]; }
     static constexpr size_t grad_stage_bytes() { return (size_t)(256 / 32) * stage_bytes_per_warp<T, LANES>(); }
-    size_t stage_bytes() const { return (size_t)(BLOCK / 32) * (sizeof(T) == 4 ? var().stage32 : var().stage64); }
+    size_t stage_bytes() const { return (size_t)(var().blk / 32) * (sizeof(T) == 4 ? var().stage32 : var().stage64); }
     void* step_kernel() const { return (sizeof(T) == 4 ? var().f32 : var().f64)(one_chunk(), split); }
     void* grad_kernel() const {
         return nth <= LANES * SLOTS ? (void*)k_gradients<T, LANES, SLOTS, true> : (void*)k_gradients<T, LANES, SLOTS, false>;
@@ -514,12 +515,13 @@ struct Engine final : EngineBase {
         CUDA_TRY(cudaFuncSetAttribute(step_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         CUDA_TRY(cudaFuncSetAttribute(grad_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_stage_bytes()));
         int per_sm = 0;
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_kernel(), BLOCK, smem));
+        const int blk = var().blk;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_kernel(), blk, smem));
         if (per_sm < 1) return fail(FCC_ERR_UNSUPPORTED, "step kernel does not fit on an SM");
         const int maxblocks = per_sm * nsm;
         const int bpw = 32 / var().L;
         const int64_t groups = (N + bpw - 1) / bpw;
-        const int64_t want = std::max<int64_t>(1, (groups + BLOCK / 32 - 1) / (BLOCK / 32));
+        const int64_t want = std::max<int64_t>(1, (groups + blk / 32 - 1) / (blk / 32));
         step_grid = (int)std::min<int64_t>(want, maxblocks);
         return FCC_OK;
     }
@@ -614,7 +616,7 @@ struct Engine final : EngineBase {
         DevPtrs<T> d = ptrs();
         int p0 = par();
         void* args[] = {&d, &nsteps, &p0};
-        CUDA_TRY(cudaLaunchCooperativeKernel(step_kernel(), dim3(step_grid), dim3(BLOCK), args, stage_bytes(), stream));
+        CUDA_TRY(cudaLaunchCooperativeKernel(step_kernel(), dim3(step_grid), dim3(var().blk), args, stage_bytes(), stream));
         gstep += nsteps;
         ++last_launches;
         return FCC_OK;
