@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <set>
 #include <string>
 #include <utility>
@@ -1076,6 +1077,8 @@ fcc_status build_neighbors_t(int64_t n, const double* x, const double* y, const 
 }
 
 }  // namespace
+
+#include "fcc_noalloc.cu"
 
 struct fcc_sim {
     std::unique_ptr<EngineBase> impl;

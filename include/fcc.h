@@ -215,6 +215,29 @@ fcc_status fcc_build_neighbors(int32_t precision, int64_t n, const double* x, co
                                int32_t cap, int32_t* cellid, int32_t* perm, int32_t* start,
                                int32_t* stop, int32_t* idx, int32_t* count);
 
+/* Neighbour build that allocates no device memory (no counterpart in the
+ * reference, which allocates its lists itself).  For callers that cannot call
+ * cudaMalloc — inside stream capture, under a memory pool or allocator they do
+ * not own, or with a device-memory budget fixed up front — this does what
+ * fcc_build_neighbors does, but on arrays already on the device: inputs x, y,
+ * rmax (n values, float for precision 32, double for 64) and outputs cellid,
+ * perm, count (n), start, stop (ncx*ncy) and idx (cap x n), in the same 1-based
+ * layout.  All other scratch lives in one static device array of this
+ * library, about 3.6 MB, which every GPU that loads the library holds until
+ * the process exits; sizes beyond FCC_NOALLOC_MAX_BODIES bodies or
+ * FCC_NOALLOC_MAX_CELLS grid cells return FCC_ERR_ARGUMENT.  Work is queued
+ * on `stream` (a cudaStream_t; NULL: the default stream) and the call returns
+ * without synchronising.  The first call on a device looks up the scratch
+ * array's device address (make that first call before any stream capture).
+ * Every call reuses the same scratch, so calls that overlap on the GPU (other
+ * streams, other threads) race: serialise them. */
+#define FCC_NOALLOC_MAX_BODIES 16384
+#define FCC_NOALLOC_MAX_CELLS 16384
+fcc_status fcc_build_neighbors_noalloc(int32_t precision, int64_t n, const void* x, const void* y, const void* rmax,
+                                       double Lx, double Ly, double cutoff, double range, int32_t cap,
+                                       int32_t* cellid, int32_t* perm, int32_t* start, int32_t* stop, int32_t* idx,
+                                       int32_t* count, void* stream);
+
 /* Device timing of the last fcc_step/fcc_run call (CUDA events on the handle's
  * stream): elapsed milliseconds, launches of this library's kernels, and
  * steps executed. */

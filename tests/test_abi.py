@@ -37,7 +37,7 @@ def test_library_exports_every_declared_symbol():
 def test_oracle_exports_mirror():
     lib = oracle.library()
     for n in declared_functions():
-        if n in ("fcc_run", "fcc_last_timing", "fcc_version"):
+        if n in ("fcc_run", "fcc_last_timing", "fcc_version", "fcc_build_neighbors_noalloc"):
             continue
         assert hasattr(lib, "fcco_" + n[4:]), n
 
