@@ -134,6 +134,26 @@ def algorithmic_per_body_step(tests_per_body, hits_per_body, nθ=40, ncoef=19, K
     return flops, bytes_
 
 
+# ------------------------------------------------------------ replicas
+def replica_seed(rank):
+    """Every rank runs an independent monolayer of its own seed."""
+    return 1234 + rank
+
+
+def max_over_ranks(x, dist=None, device="cpu"):
+    """Job time = the slowest rank's time (all ranks take this collective)."""
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, n_bodies, steps, seconds):
+    """Body-steps/s of the whole job: every rank's bodies over the slowest time."""
+    return world * n_bodies * steps / seconds
+
+
 def flush_l2():
     import torch
     buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
@@ -214,7 +234,7 @@ def gpu_arm(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
     fcc = load_package()
-    bodies, box, kw = workload(fcc, seed=1234 + rank)
+    bodies, box, kw = workload(fcc, seed=replica_seed(rank))
     sim = fcc.Simulation(bodies, box, T=np.float32, **kw)
     N = bodies.n
 
@@ -230,11 +250,8 @@ def gpu_arm(args):
     ms, launches, steps = sim.last_timing()
     if dist:
         dist.barrier()
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * N * steps / (ms_max * 1e-3)
+    ms_max = max_over_ranks(ms, dist, "cuda")
+    value = job_throughput(world, N, steps, ms_max * 1e-3)
 
     # end to end through the C ABI with host buffers (wall clock, max over ranks)
     host = sim.bodies
@@ -249,10 +266,7 @@ def gpu_arm(args):
     out = sim.bodies
     e2e_s = time.perf_counter() - t0
     assert np.isfinite(out.x).all()
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e = world * N * args.steps / float(te.item())
+    e2e = job_throughput(world, N, args.steps, max_over_ranks(e2e_s, dist, "cuda"))
 
     if rank == 0:
         peaks = {}
