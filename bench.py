@@ -162,6 +162,73 @@ def flush_l2():
     del buf
 
 
+# ------------------------------------------------------------ batching
+BATCH_WORKLOAD = ("256 monolayers, N log-uniform on [64, 4096] (square-ish hexagonal packings at 0.95, "
+                  "R0 ~ N(1, 0.1) clipped to [0.8, 1.2]), v0 ~ U[0.02, 0.2], eta log-uniform on [0.001, 0.1], "
+                  "Tension(eta) + Overlap(1.0), Dr 0.01, mu_ab 0.1, dt 0.005, 2000 steps each, FP32")
+
+
+def batch_members(fcc, count=256, nmin=64, nmax=4096, seed=2024):
+    """The batching workload: `count` independent monolayers of uneven N."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n_t = math.exp(rng.uniform(math.log(nmin), math.log(nmax)))
+        ny = max(2, 2 * round(math.sqrt(2 * n_t / math.sqrt(3)) / 2))  # Lx ~ Ly
+        nx = max(1, round(n_t / ny))
+        v0 = float(rng.uniform(0.02, 0.2))
+        eta = float(math.exp(rng.uniform(math.log(1e-3), math.log(0.1))))
+        sd = int(rng.integers(1, 2**31 - 1))
+        bodies, box = fcc.polydisperse_monolayer(nx, ny, packing=0.95, maxmode=10, seed=sd)
+        kw = dict(types=(fcc.BodyType(v0=v0, Dr=0.01, μab=0.1),), energies=(fcc.Tension(eta), fcc.Overlap(1.0)),
+                  dt=0.005, seed=sd)
+        out.append((bodies, box, kw))
+    return out
+
+
+def batched_leg(fcc, steps=2000, warm=3, count=256):
+    """Batched (one pool, one persistent launch per 512 steps for all 256
+    monolayers) against the plain per-simulation loop (each monolayer run
+    alone, one after the other), on the same inputs; device-timed."""
+    import torch
+    members = batch_members(fcc, count)
+    total = sum(b.n for b, _, _ in members)
+    cells = sum(fcc.pool.grid_cells(box, b.R0, T=np.float32) for b, box, _ in members)
+    pool = fcc.Pool(T=np.float32, max_bodies=sum(fcc.pool.padded(b.n) for b, _, _ in members),
+                    max_cells=cells, max_sims=count)
+    slots = [pool.add(b, box, horizon=warm + steps, **kw) for b, box, kw in members]
+    pool.run(warm)
+    flush_l2()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pool.run(steps)
+    wall_b = time.perf_counter() - t0
+    ms_b, launches_b, bsteps = pool.last_timing()
+    var = pool.variant()
+    # plain loop
+    ms_p, wall_p, equal = 0.0, 0.0, 0
+    for (b, box, kw), slot in zip(members, slots):
+        sim = fcc.Simulation(b, box, T=np.float32, **kw)
+        sim.run(warm)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.run(steps)
+        wall_p += time.perf_counter() - t0
+        ms_p += sim.last_timing()[0]
+        a, c = sim.bodies, pool.bodies(slot)
+        equal += int(all(np.array_equal(getattr(a, f), getattr(c, f)) for f in ("x", "y", "θ", "coef", "imgx")))
+        sim.close()
+    pool.close()
+    vb = total * steps / (ms_b * 1e-3)
+    vp = total * steps / (ms_p * 1e-3)
+    return {"workload": BATCH_WORKLOAD, "sims": count, "bodies": total, "steps": steps,
+            "batched": {"value": vb, "unit": "body-steps/s", "ms": ms_b, "launches": launches_b,
+                        "wall_value": total * steps / wall_b, "kernel": var},
+            "plain": {"value": vp, "unit": "body-steps/s", "ms": ms_p, "wall_value": total * steps / wall_p},
+            "batched_over_plain": vb / vp,
+            "bitwise_equal_to_plain": f"{equal}/{count}"}
+
+
 # ------------------------------------------------------------------ arms
 def cpu_baseline(fcc, oracle, budget_s=15.0, max_steps=200):
     """The oracle (FP64, OpenMP on all host cores) on the same workload,
@@ -297,6 +364,7 @@ def gpu_arm(args):
         fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
         achieved_tf = flops_b * N * steps_per_launch / (launch_ms * 1e-3) / 1e12
         cpu, _ = cpu_baseline(fcc, oracle)
+        batched = batched_leg(fcc) if not args.skip_batched else None
         line = {
             "metric": METRIC, "value": value, "unit": "body-steps/s", "n_gpus": world, "steps": steps,
             "warmup": args.warmup, "ms_per_step": ms_max / steps, "higher_is_better": True, "scaling": "weak",
@@ -319,6 +387,7 @@ def gpu_arm(args):
             "gpu_launches": launches * world,
             "clocks": cs,
             "builds": sim.builds,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if dist:
@@ -332,6 +401,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--warmup", type=int, default=200)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--skip-batched", action="store_true", help="leave out the batching leg")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

@@ -13,7 +13,7 @@ The directory name is not a Python identifier; load it with
 ``__graft_entry__.py``).
 """
 
-from .model import (ArgumentError, DimensionMismatch, DeviceError, BodyType, EnergyTerm, BodyTerm, ContactTerm,
+from .model import (ArgumentError, DimensionMismatch, DeviceError, PoolFull, BodyType, EnergyTerm, BodyTerm, ContactTerm,
                     BondTerm, Tension, PerimeterElasticity, Overlap, LinearRepulsion, HarmonicBond, OnTypes,
                     Bodies, PeriodicBox, vcat, nbodies, hexagonal_monolayer, with_nuclei, parent_bonds,
                     polydisperse_monolayer, minimum_image, wrap)
@@ -21,9 +21,10 @@ from .simulation import (Simulation, NativeSimulation, native_library, step, run
                          update_neighbors, perimeters, areas, shape_index, body_energy, positions,
                          unwrapped_positions, contours, protrusion, Gradients, Geometry, NeighborInfo)
 from .ops import philox_noise, build_neighbors
+from .pool import Pool
 
 __all__ = [
-    "ArgumentError", "DimensionMismatch", "DeviceError", "BodyType", "EnergyTerm", "BodyTerm", "ContactTerm",
+    "ArgumentError", "DimensionMismatch", "DeviceError", "PoolFull", "Pool", "BodyType", "EnergyTerm", "BodyTerm", "ContactTerm",
     "BondTerm", "Tension", "PerimeterElasticity", "Overlap", "LinearRepulsion", "HarmonicBond", "OnTypes",
     "Bodies", "PeriodicBox", "vcat", "nbodies", "hexagonal_monolayer", "with_nuclei", "parent_bonds",
     "polydisperse_monolayer", "minimum_image", "wrap", "Simulation", "NativeSimulation", "native_library", "step",

@@ -13,7 +13,7 @@ import ctypes as C
 
 import numpy as np
 
-from .model import (ArgumentError, DimensionMismatch, DeviceError, BodyType, Bodies, OnTypes, Tension,
+from .model import (ArgumentError, DimensionMismatch, DeviceError, PoolFull, BodyType, Bodies, OnTypes, Tension,
                     PerimeterElasticity, Overlap, LinearRepulsion, HarmonicBond, is_body_term,
                     is_contact_term, is_bond_term)
 
@@ -21,7 +21,9 @@ MAX_TYPES = 8
 MAX_TERMS = 16
 MAX_MODES = 9
 
-FCC_OK, FCC_ERR_ARGUMENT, FCC_ERR_DIMENSION, FCC_ERR_CUDA, FCC_ERR_UNSUPPORTED, FCC_ERR_DEVICE, FCC_ERR_NOMEM = range(7)
+(FCC_OK, FCC_ERR_ARGUMENT, FCC_ERR_DIMENSION, FCC_ERR_CUDA, FCC_ERR_UNSUPPORTED, FCC_ERR_DEVICE, FCC_ERR_NOMEM,
+ FCC_ERR_FULL) = range(8)
+POOL_ALIGN = 8
 
 c_double_p = C.POINTER(C.c_double)
 c_int32_p = C.POINTER(C.c_int32)
@@ -62,6 +64,12 @@ class FccGeometryHost(C.Structure):
 
 class FccNeighborsHost(C.Structure):
     _fields_ = [(f, c_int32_p) for f in ("cellid", "perm", "start", "stop", "idx", "count")]
+
+
+class FccPoolParams(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("ntheta", C.c_int32), ("max_bodies", C.c_int64),
+                ("max_cells", C.c_int64), ("max_sims", C.c_int32), ("nl_capacity", C.c_int32),
+                ("max_children", C.c_int32), ("max_bonds", C.c_int32)]
 
 
 FCC_CALLBACK = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p)
@@ -210,6 +218,8 @@ def check(status: int, lasterr) -> None:
         raise ArgumentError(msg)
     if status == FCC_ERR_DIMENSION:
         raise DimensionMismatch(msg)
+    if status == FCC_ERR_FULL:
+        raise PoolFull(msg)
     raise DeviceError(f"status {status}: {msg}")
 
 

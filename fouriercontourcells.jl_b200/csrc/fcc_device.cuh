@@ -50,6 +50,7 @@ enum : int {
     F_ACTIVE = 16,     // slot holds a simulation
     F_NONFINITE = 32,  // a body state became non-finite
     F_CONTACT = 64,    // simulation has contact terms (uses neighbour lists)
+    F_HOLD = 128,      // reached its step limit: keeps its state until the host releases it
 };
 
 enum : int { BT_TENSION = 1, BT_PERIMETER = 2 };
@@ -113,6 +114,7 @@ struct DevPtrs {
     const int* bd_count;
     int* flags;
     long long* clock;
+    const long long* stop;  // per simulation: clock value at which it holds (null: no limit)
     long long* builds;
     int* maxcount;
     GridSync* sync;

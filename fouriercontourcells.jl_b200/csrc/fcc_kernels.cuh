@@ -201,7 +201,7 @@ template <class T>
 __device__ void phase_count(const DevPtrs<T>& d, int par, int tid, int nthr) {
     for (int g = tid; g < d.Ntot; g += nthr) {
         const int s = __ldg(d.sim_of + g);
-        if (!(ldcg(d.flags + s) & F_NEED)) continue;
+        if (s < 0 || !(ldcg(d.flags + s) & F_NEED)) continue;
         const SimDesc<T>& P = d.sims[s];
         const T* r = rec_cur(d, par) + (size_t)g * RECW;
         int cx, cy;
@@ -272,7 +272,7 @@ template <class T>
 __device__ void phase_scatter(const DevPtrs<T>& d, int tid, int nthr) {
     for (int g = tid; g < d.Ntot; g += nthr) {
         const int s = __ldg(d.sim_of + g);
-        if (!(ldcg(d.flags + s) & F_NEED)) continue;
+        if (s < 0 || !(ldcg(d.flags + s) & F_NEED)) continue;
         d.perm[ldcg(d.cstart + ldcg(d.cellid + g)) + ldcg(d.slot + g)] = g;
     }
 }
@@ -304,7 +304,7 @@ template <class T>
 __device__ void phase_neighbors(const DevPtrs<T>& d, int par, int tid, int nthr) {
     for (int g = tid; g < d.Ntot; g += nthr) {
         const int s = __ldg(d.sim_of + g);
-        if (!(ldcg(d.flags + s) & F_NEED)) continue;
+        if (s < 0 || !(ldcg(d.flags + s) & F_NEED)) continue;
         const SimDesc<T>& P = d.sims[s];
         const T* rc = rec_cur(d, par);
         const T xi = ldcg(rc + (size_t)g * RECW + R_X), yi = ldcg(rc + (size_t)g * RECW + R_Y);
@@ -597,15 +597,23 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
     const int lane = threadIdx.x & 31;
     const int l = lane & (L - 1);
     const int g = wg * BPW + lane / L;
-    const bool valid = g < d.Ntot;
-    const int gg = valid ? g : 0;
+    // Several simulations: each one's bodies start at a multiple of 8 and its
+    // padding follows them, so a warp group lies in one simulation and its
+    // first body is real unless the whole group is padding.
+    int s = 0;
+    if (!sim0) {
+        const int gf = wg * BPW;
+        s = gf < d.Ntot ? __ldg(d.sim_of + gf) : -1;
+        if (s < 0) return;
+    }
+    const SimDesc<T>& P = sim0 ? *sim0 : d.sims[s];
+    const bool valid = sim0 ? g < d.Ntot : g < P.body_off + P.n;
+    const int gg = valid ? g : (sim0 ? 0 : wg * BPW);
     const T* rc = rec_cur(d, par);
     // ---- independent loads first: own record, neighbour count and ids,
     // simulation state, update operands
     T rv[RECW];
     load_rec(rc + (size_t)gg * RECW, rv);
-    const int s = sim0 ? 0 : __ldg(d.sim_of + gg);
-    const SimDesc<T>& P = sim0 ? *sim0 : d.sims[s];
     const T r0 = __ldg(d.R0 + gg);
     const int cnt_raw = ldcg(d.nb_count + gg);
     int ids[IDS];
@@ -619,7 +627,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
     UpdatePre<T, L> pre;
     if (MODE == MODE_FUSED) load_update_pre(d, gg, l, P.K, pre);
     bool act = valid;
-    if (MODE != MODE_DIAG) act = act && (fl & F_ACTIVE) && !(fl & F_FROZEN);
+    if (MODE != MODE_DIAG) act = act && (fl & F_ACTIVE) && !(fl & (F_FROZEN | F_HOLD));
     const int nth = P.nth;
     const T dphi = P.dphi;
 
@@ -949,12 +957,17 @@ __device__ __forceinline__ void update_warp_split(const DevPtrs<T>& d, int wg, i
     const int lane = threadIdx.x & 31;
     const int l = lane & (L - 1);
     const int g = wg * BPW + lane / L;
-    const bool valid = g < d.Ntot;
-    const int gg = valid ? g : 0;
-    const int s = sim0 ? 0 : __ldg(d.sim_of + gg);
-    const int fl = ldcg(d.flags + s);
-    const bool act = valid && (fl & F_ACTIVE) && !(fl & F_FROZEN);
+    int s = 0;
+    if (!sim0) {
+        const int gf = wg * BPW;
+        s = gf < d.Ntot ? __ldg(d.sim_of + gf) : -1;
+        if (s < 0) return;
+    }
     const SimDesc<T>& P = sim0 ? *sim0 : d.sims[s];
+    const bool valid = sim0 ? g < d.Ntot : g < P.body_off + P.n;
+    const int gg = valid ? g : (sim0 ? 0 : wg * BPW);
+    const int fl = ldcg(d.flags + s);
+    const bool act = valid && (fl & F_ACTIVE) && !(fl & (F_FROZEN | F_HOLD));
     const long long clk = ldcg(d.clock + s);
     T rv[RECW];
     load_rec(rec_cur(d, par) + (size_t)gg * RECW, rv);
@@ -983,13 +996,20 @@ __device__ void bookkeeping(const DevPtrs<T>& d) {
     __syncthreads();
     for (int s = threadIdx.x; s < d.nsims; s += blockDim.x) {
         int f = ldcg(d.flags + s);
-        if ((f & F_ACTIVE) && !(f & F_FROZEN)) {
-            d.clock[s] = ldcg(d.clock + s) + 1;
-            const bool need = (f & F_CONTACT) && ((f & F_REBUILD) || !(f & F_VALID) || d.sims[s].skin == T(0));
-            f &= ~(F_REBUILD | F_NEED);
-            if (need) {
-                f |= F_NEED;
-                s_any = 1;
+        if ((f & F_ACTIVE) && !(f & (F_FROZEN | F_HOLD))) {
+            const long long c = ldcg(d.clock + s) + 1;
+            d.clock[s] = c;
+            if (d.stop && c >= ldcg(d.stop + s)) {
+                // step limit reached: hold; F_REBUILD stays for the host's
+                // rebuild decision when it releases the simulation
+                f = (f & ~F_NEED) | F_HOLD;
+            } else {
+                const bool need = (f & F_CONTACT) && ((f & F_REBUILD) || !(f & F_VALID) || d.sims[s].skin == T(0));
+                f &= ~(F_REBUILD | F_NEED);
+                if (need) {
+                    f |= F_NEED;
+                    s_any = 1;
+                }
             }
         } else {
             f &= ~F_NEED;
@@ -1103,6 +1123,7 @@ __global__ void k_skin_check(DevPtrs<T> d, int par) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= d.Ntot) return;
     const int s = __ldg(d.sim_of + g);
+    if (s < 0) return;
     const int f = ldcg(d.flags + s);
     if (!(f & F_CONTACT) || !(f & F_VALID)) return;
     const SimDesc<T>& P = d.sims[s];
@@ -1157,17 +1178,19 @@ __global__ void k_finish_rebuild(DevPtrs<T> d) {
 // Simulation set-up and set_state: enforce_shape! (FP64 sums) and the lab
 // frame of the given body state into rec[par] (src/simulation.jl:102-103,
 // src/dynamics.jl:44-64, src/geometry.jl:208-227).  One thread per body.
+// Bodies g0 .. g0+n-1; the inputs are indexed from g0.
 template <class T>
-__global__ void k_init(DevPtrs<T> d, int par, const T* __restrict__ x, const T* __restrict__ y,
+__global__ void k_init(DevPtrs<T> d, int par, int g0, int n, const T* __restrict__ x, const T* __restrict__ y,
                        const T* __restrict__ th, const T* __restrict__ coef_in) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= d.Ntot) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int g = g0 + i;
     const int s = d.sim_of[g];
     const SimDesc<T>& P = d.sims[s];
     const int K = P.K;
     T c[NCM];
 #pragma unroll
-    for (int r = 0; r < NCM; ++r) c[r] = coef_in[(size_t)g * NCM + r];
+    for (int r = 0; r < NCM; ++r) c[r] = coef_in[(size_t)i * NCM + r];
     double ssum = 0.0;
     for (int m = 0; m < K; ++m) ssum += sqrt((double)c[1 + m] * c[1 + m] + (double)c[1 + KM + m] * c[1 + KM + m]);
     if (ssum > SHAPE_BOUND) {
@@ -1189,7 +1212,7 @@ __global__ void k_init(DevPtrs<T> d, int par, const T* __restrict__ x, const T* 
         T al = T(0), be = T(0);
         if (m < K) {
             T so, co;
-            t_sincos(T(m + 2) * th[g], &so, &co);
+            t_sincos(T(m + 2) * th[i], &so, &co);
             al = c[1 + m] * co - c[1 + KM + m] * so;
             be = c[1 + m] * so + c[1 + KM + m] * co;
             bound += t_sqrt(c[1 + m] * c[1 + m] + c[1 + KM + m] * c[1 + KM + m]);
@@ -1197,22 +1220,22 @@ __global__ void k_init(DevPtrs<T> d, int par, const T* __restrict__ x, const T* 
         rn[r_al(m)] = r0 * al;
         rn[r_be(m)] = r0 * be;
     }
-    rn[R_X] = x[g];
-    rn[R_Y] = y[g];
+    rn[R_X] = x[i];
+    rn[R_Y] = y[i];
     rn[R_RMAX] = r0 * bound;
     rn[R_A0] = r0 * c[0];  // R_W (parent, type) is written by k_set_w
-    rn[R_TH] = th[g];
+    rn[R_TH] = th[i];
 #pragma unroll
     for (int r = 0; r < NCM; ++r) d.coef[(size_t)g * NCM + r] = c[r];
 }
 
 // w field (parent, type) of the current record
 template <class T>
-__global__ void k_set_w(DevPtrs<T> d, int par, const int* __restrict__ w) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= d.Ntot) return;
+__global__ void k_set_w(DevPtrs<T> d, int par, int g0, int n, const int* __restrict__ w) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
     T* tag = nullptr;
-    rec_cur_mut(d, par)[(size_t)g * RECW + R_W] = pack_w(w[g], tag);
+    rec_cur_mut(d, par)[(size_t)(g0 + i) * RECW + R_W] = pack_w(w[i], tag);
 }
 
 // Geometry of the current state for get_geometry: lab, labR0, rmax, and
@@ -1223,6 +1246,7 @@ __global__ void k_geometry(DevPtrs<T> d, int par, T* lab, T* labR0, T* R, T* dR,
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= d.Ntot) return;
     const int s = d.sim_of[g];
+    if (s < 0) return;
     const SimDesc<T>& P = d.sims[s];
     const T* rc = rec_cur(d, par) + (size_t)g * RECW;
     const T* cf = d.coef + (size_t)g * NCM;
@@ -1265,11 +1289,14 @@ __global__ void k_geometry(DevPtrs<T> d, int par, T* lab, T* labR0, T* R, T* dR,
 }
 
 // perimeters, areas, shape index with FP64 node sums (src/observables.jl:7-18).
+// Bodies g0 .. g0+n-1, out indexed from g0.
 template <class T>
-__global__ void k_observables(DevPtrs<T> d, int par, double* out) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= d.Ntot) return;
+__global__ void k_observables(DevPtrs<T> d, int par, int g0, int n, double* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int g = g0 + i;
     const int s = d.sim_of[g];
+    if (s < 0) return;
     const SimDesc<T>& P = d.sims[s];
     const T* rc = rec_cur(d, par) + (size_t)g * RECW;
     double per = 0.0, area = 0.0;
@@ -1290,9 +1317,9 @@ __global__ void k_observables(DevPtrs<T> d, int par, double* out) {
     }
     per *= (double)P.dphi;
     area *= (double)P.dphi / 2.0;
-    out[3 * (size_t)g] = per;
-    out[3 * (size_t)g + 1] = area;
-    out[3 * (size_t)g + 2] = per / sqrt(area);
+    out[3 * (size_t)i] = per;
+    out[3 * (size_t)i + 1] = area;
+    out[3 * (size_t)i + 2] = per / sqrt(area);
 }
 
 // philox_noise! (src/random.jl:113-130): first three normals of body i.

@@ -110,6 +110,244 @@ const Variant VARIANTS[] = {
 constexpr int NVARIANTS = sizeof(VARIANTS) / sizeof(VARIANTS[0]);
 constexpr int LANES = 8, SLOTS = 5;  // compute_gradients and the FP64 step
 
+// A simulation as set up from the reference's constructor arguments
+// (src/simulation.jl:66-105), validated and converted to T, with local body
+// ids: the part of an engine that does not depend on where its bodies sit.
+template <class T>
+struct SimSpec {
+    SimDesc<T> desc{};  // body_off = cell_off = 0
+    int64_t N = 0;
+    int K = 0, nc = 0, nth = 0, ncx = 1, ncy = 1;
+    bool has_contact = false, split = false;
+    std::vector<int32_t> type, parent;
+    std::vector<T> R0;
+    std::vector<int> chc, chi, bdc, bdi;  // children and bond partners per body (local ids)
+    int ccap = 1, bcap = 1;
+};
+
+template <class T>
+fcc_status make_spec(const fcc_params* p, const fcc_bodies_host* b, SimSpec<T>& sp) {
+    // validation in the order of src/simulation.jl:66-105
+    if (!p || !b) return fail(FCC_ERR_ARGUMENT, "null argument");
+    if (p->ntypes < 1 || p->ntypes > FCC_MAX_TYPES || !p->types)
+        return fail(FCC_ERR_ARGUMENT, "types must hold 1..8 BodyType entries");
+    for (int t = 0; t < p->ntypes; ++t)
+        if (p->types[t].parent_drag != 0 && p->types[t].parent_drag != 1)
+            return fail(FCC_ERR_ARGUMENT, "drag must be :substrate or :parent");
+    if (p->nterms < 0 || p->nterms > FCC_MAX_TERMS || (p->nterms > 0 && !p->terms))
+        return fail(FCC_ERR_ARGUMENT, "energy terms must be BodyTerms, ContactTerms or BondTerms");
+    for (int q = 0; q < p->nterms; ++q) {
+        const fcc_term& ft = p->terms[q];
+        if (ft.kind < FCC_TENSION || ft.kind > FCC_HARMONIC_BOND)
+            return fail(FCC_ERR_ARGUMENT, "energy terms must be BodyTerms, ContactTerms or BondTerms");
+        if (ft.ntypes_on < 0 || ft.ntypes_on > FCC_MAX_TYPES) return fail(FCC_ERR_ARGUMENT, "OnTypes: bad type list");
+        if (ft.kind == FCC_OVERLAP && (ft.nJ < 1 || ft.nJ > FCC_MAX_TYPES))
+            return fail(FCC_ERR_DIMENSION, "coupling tables must be square and equal-sized");
+    }
+    int64_t& N = sp.N;
+    N = b->n;
+    if (N < 0) return fail(FCC_ERR_DIMENSION, "inconsistent body array lengths");
+    if (N > (1 << 27)) return fail(FCC_ERR_UNSUPPORTED, "at most 2^27 bodies per simulation");
+    int32_t maxtype = 0;
+    for (int64_t i = 0; i < N; ++i) {
+        if (b->type[i] > p->ntypes) return fail(FCC_ERR_ARGUMENT, "body type without BodyType entry");
+        if (b->type[i] < 1) return fail(FCC_ERR_ARGUMENT, "body type ids are 1-based");
+        maxtype = std::max(maxtype, b->type[i]);
+    }
+    for (int q = 0; q < p->nterms; ++q) {
+        const fcc_term& ft = p->terms[q];
+        if (ft.kind == FCC_OVERLAP && ft.nJ > 1 && ft.nJ < maxtype)
+            return fail(FCC_ERR_DIMENSION, "Overlap coupling table smaller than the number of body types");
+    }
+    for (int64_t i = 0; i < N; ++i) {  // check_parents, src/simulation.jl:108-118
+        int64_t pp = b->parent[i];
+        if (pp < 1 || pp > N)
+            return fail(FCC_ERR_ARGUMENT, "body " + std::to_string(i + 1) + " has parent " + std::to_string(pp) +
+                                              " outside 1:" + std::to_string(N));
+        if (!p->types[b->type[i] - 1].parent_drag) continue;
+        if (pp == i + 1)
+            return fail(FCC_ERR_ARGUMENT, "body " + std::to_string(i + 1) + " has drag = :parent but is its own parent");
+        if (p->types[b->type[pp - 1] - 1].parent_drag)
+            return fail(FCC_ERR_ARGUMENT, "body " + std::to_string(i + 1) + " has drag = :parent, but so has its parent " +
+                                              std::to_string(pp) + " (one level only)");
+    }
+    int& K = sp.K;
+    int& nth = sp.nth;
+    int& nc = sp.nc;
+    K = b->ncoef / 2;
+    nth = p->ntheta;
+    if (K + 1 < 2) return fail(FCC_ERR_ARGUMENT, "maxmode must be ≥ 2");
+    if (!(nth > 2 * (K + 1))) return fail(FCC_ERR_ARGUMENT, "nθ must exceed 2·maxmode");
+    nc = 2 * K + 1;
+    if (b->ncoef != nc) return fail(FCC_ERR_DIMENSION, "coefficient rows must be odd: [a₀; aₙ; bₙ]");
+    if (K > KM) return fail(FCC_ERR_UNSUPPORTED, "this build supports maxmode ≤ 10");
+    if (!(p->skin >= 0)) return fail(FCC_ERR_ARGUMENT, "skin must be non-negative");
+
+    // simulation descriptor (convert_precision: every parameter to T)
+    SimDesc<T>& s = sp.desc;
+    s = SimDesc<T>{};
+    std::vector<T>& R0_h = sp.R0;
+    int& ncx = sp.ncx;
+    int& ncy = sp.ncy;
+    bool& has_contact = sp.has_contact;
+    bool& split = sp.split;
+    has_contact = false;
+    s.Lx = (T)p->Lx;
+    s.Ly = (T)p->Ly;
+    s.invLx = T(1) / s.Lx;
+    s.invLy = T(1) / s.Ly;
+    s.dt = (T)p->dt;
+    s.skin = (T)p->skin;
+    s.crange = T(0);  // interaction_range of the built-in contact terms
+    s.nbrange = s.crange + s.skin;
+    s.dphi = (T)(2 * PI / nth);
+    R0_h.resize(N);
+    double maxR0 = 0;
+    for (int64_t i = 0; i < N; ++i) {
+        R0_h[i] = (T)b->R0[i];
+        maxR0 = std::max(maxR0, (double)R0_h[i]);
+    }
+    const double cutoff = 2 * maxR0 * (1 + SHAPE_BOUND) + 0.0 + p->skin;  // src/simulation.jl:90
+    auto ncells = [&](T L) {
+        int64_t n = (int64_t)std::floor((double)L / cutoff);
+        return (int)(n >= 3 ? n : 1);
+    };
+    ncx = ncells(s.Lx);
+    ncy = ncells(s.Ly);
+    if ((int64_t)ncx * ncy > (1 << 28)) return fail(FCC_ERR_UNSUPPORTED, "cell grid too large");
+    s.wx = s.Lx / (T)ncx;
+    s.wy = s.Ly / (T)ncy;
+    s.ncx = ncx;
+    s.ncy = ncy;
+    s.cell_off = 0;
+    s.ncells = ncx * ncy;
+    s.body_off = 0;
+    s.n = (int)N;
+    s.nth = nth;
+    s.K = K;
+    s.k0 = (uint32_t)(p->seed & 0xffffffffu);
+    s.k1 = (uint32_t)(p->seed >> 32);
+    s.ntypes = p->ntypes;
+    s.rewrap = (ncx < 3 || ncy < 3) ? 1 : 0;
+    for (int t = 0; t < p->ntypes; ++t) {
+        const fcc_body_type& bt = p->types[t];
+        s.v0[t] = (T)bt.v0;
+        s.Dr[t] = (T)bt.Dr;
+        s.Dt[t] = (T)bt.Dt;
+        s.mur[t] = (T)bt.mu_r;
+        s.muth[t] = (T)bt.mu_theta;
+        s.muab[t] = (T)bt.mu_ab;
+        s.parent_drag[t] = bt.parent_drag;
+    }
+    auto mask_of = [](const fcc_term& ft) {
+        if (ft.ntypes_on == 0) return 0xffffffffu;
+        uint32_t m = 0;
+        for (int u = 0; u < ft.ntypes_on; ++u)
+            if (ft.types_on[u] >= 1 && ft.types_on[u] <= FCC_MAX_TYPES) m |= 1u << (ft.types_on[u] - 1);
+        return m;
+    };
+    // contact couplings summed over terms in the reference's order g1 + (g2 + ...)
+    for (int r = 0; r < 2; ++r)
+        for (int a = 0; a < MT; ++a)
+            for (int c = 0; c < MT; ++c) s.cA[r][a][c] = T(0);
+    for (int a = 0; a < MT; ++a) s.cB[a] = T(0);
+    for (int q = p->nterms - 1; q >= 0; --q) {
+        const fcc_term& ft = p->terms[q];
+        const uint32_t mk = mask_of(ft);
+        if (ft.kind == FCC_OVERLAP) {
+            has_contact = true;
+            for (int a = 0; a < MT; ++a) {
+                if (!((mk >> a) & 1u)) continue;
+                for (int c = 0; c < MT; ++c) {
+                    const int ij = ft.nJ == 1 ? 0 : (a < ft.nJ && c < ft.nJ ? a + ft.nJ * c : -1);
+                    if (ij < 0) continue;
+                    s.cA[0][a][c] = (T)ft.J[ij] + s.cA[0][a][c];
+                    s.cA[1][a][c] = (T)ft.Jrel[ij] + s.cA[1][a][c];
+                }
+            }
+        } else if (ft.kind == FCC_LINEAR_REPULSION) {
+            has_contact = true;
+            for (int a = 0; a < MT; ++a)
+                if ((mk >> a) & 1u) s.cB[a] = (T)ft.a + s.cB[a];
+        }
+    }
+    s.nbt = 0;
+    s.nbd = 0;
+    for (int q = 0; q < p->nterms; ++q) {
+        const fcc_term& ft = p->terms[q];
+        if (ft.kind == FCC_TENSION || ft.kind == FCC_PERIMETER_ELASTICITY) {
+            const int u = s.nbt++;
+            s.bt_kind[u] = ft.kind == FCC_TENSION ? BT_TENSION : BT_PERIMETER;
+            s.bt_mask[u] = mask_of(ft);
+            s.bt_a[u] = (T)ft.a;
+            // l0 = p0 * sqrt(π) * R0 (src/energies/body_terms.jl:34)
+            s.bt_b[u] = ft.kind == FCC_TENSION ? T(0) : (T)ft.b * std::sqrt((T)PI);
+        } else if (ft.kind == FCC_HARMONIC_BOND) {
+            const int u = s.nbd++;
+            s.bd_mask[u] = mask_of(ft);
+            s.bd_k[u] = (T)ft.a;
+            s.bd_r0[u] = (T)ft.b;
+        }
+    }
+    s.has_contact = has_contact ? 1 : 0;
+    s.has_noise = 0;
+    for (int t = 0; t < p->ntypes; ++t)
+        if (p->types[t].Dr != 0 || p->types[t].Dt != 0) s.has_noise = 1;
+    split = false;
+    for (int64_t i = 0; i < N; ++i)
+        if (p->types[b->type[i] - 1].parent_drag) split = true;
+    s.has_parent_drag = split ? 1 : 0;
+
+    // children (src/bodies.jl:121-135) and bonds (src/energies/bonds.jl:52-71), local ids
+    std::vector<int32_t>& type_h = sp.type;
+    std::vector<int32_t>& parent_h = sp.parent;
+    type_h.assign(b->type, b->type + N);
+    parent_h.assign(b->parent, b->parent + N);
+    std::vector<int>& chc = sp.chc;
+    chc.assign(N, 0);
+    for (int64_t k = 0; k < N; ++k)
+        if (parent_h[k] != k + 1) chc[parent_h[k] - 1] += 1;
+    int& ccap = sp.ccap;
+    ccap = 1;
+    for (int64_t k = 0; k < N; ++k) ccap = std::max(ccap, chc[k]);
+    std::vector<int>& chi = sp.chi;
+    chi.assign((size_t)ccap * N, 0);
+    std::fill(chc.begin(), chc.end(), 0);
+    for (int64_t k = 0; k < N; ++k) {
+        const int pp = parent_h[k] - 1;
+        if (pp == k) continue;
+        chi[(size_t)pp * ccap + chc[pp]++] = (int)k;
+    }
+    std::vector<int>& bdc = sp.bdc;
+    bdc.assign(N, 0);
+    std::set<std::pair<int64_t, int64_t>> seen;
+    for (int64_t q = 0; q < p->nbonds; ++q) {
+        const int64_t i = p->bonds[2 * q], j = p->bonds[2 * q + 1];
+        if (!(1 <= i && i <= N && 1 <= j && j <= N))
+            return fail(FCC_ERR_ARGUMENT, "bond (" + std::to_string(i) + ", " + std::to_string(j) +
+                                              ") refers to a body outside 1:" + std::to_string(N));
+        if (i == j)
+            return fail(FCC_ERR_ARGUMENT, "bond (" + std::to_string(i) + ", " + std::to_string(j) + ") connects a body to itself");
+        auto key = std::make_pair(std::min(i, j), std::max(i, j));
+        if (seen.count(key)) return fail(FCC_ERR_ARGUMENT, "duplicate bond (" + std::to_string(i) + ", " + std::to_string(j) + ")");
+        seen.insert(key);
+        bdc[i - 1] += 1;
+        bdc[j - 1] += 1;
+    }
+    int& bcap = sp.bcap;
+    bcap = 1;
+    for (int64_t k = 0; k < N; ++k) bcap = std::max(bcap, bdc[k]);
+    std::vector<int>& bdi = sp.bdi;
+    bdi.assign((size_t)bcap * N, 0);
+    std::fill(bdc.begin(), bdc.end(), 0);
+    for (int64_t q = 0; q < p->nbonds; ++q) {
+        const int64_t i = p->bonds[2 * q] - 1, j = p->bonds[2 * q + 1] - 1;
+        bdi[(size_t)i * bcap + bdc[i]++] = (int)j;
+        bdi[(size_t)j * bcap + bdc[j]++] = (int)i;
+    }
+    return FCC_OK;
+}
+
 struct EngineBase {
     virtual ~EngineBase() = default;
     virtual fcc_status step(int64_t n, bool eager) = 0;
@@ -227,58 +465,8 @@ struct Engine final : EngineBase {
 
     // ------------------------------------------------------------ set-up --
     fcc_status init(const fcc_params* p, const fcc_bodies_host* b) {
-        // validation in the order of src/simulation.jl:66-105
-        if (!p || !b) return fail(FCC_ERR_ARGUMENT, "null argument");
-        if (p->ntypes < 1 || p->ntypes > FCC_MAX_TYPES || !p->types)
-            return fail(FCC_ERR_ARGUMENT, "types must hold 1..8 BodyType entries");
-        for (int t = 0; t < p->ntypes; ++t)
-            if (p->types[t].parent_drag != 0 && p->types[t].parent_drag != 1)
-                return fail(FCC_ERR_ARGUMENT, "drag must be :substrate or :parent");
-        if (p->nterms < 0 || p->nterms > FCC_MAX_TERMS || (p->nterms > 0 && !p->terms))
-            return fail(FCC_ERR_ARGUMENT, "energy terms must be BodyTerms, ContactTerms or BondTerms");
-        for (int q = 0; q < p->nterms; ++q) {
-            const fcc_term& ft = p->terms[q];
-            if (ft.kind < FCC_TENSION || ft.kind > FCC_HARMONIC_BOND)
-                return fail(FCC_ERR_ARGUMENT, "energy terms must be BodyTerms, ContactTerms or BondTerms");
-            if (ft.ntypes_on < 0 || ft.ntypes_on > FCC_MAX_TYPES) return fail(FCC_ERR_ARGUMENT, "OnTypes: bad type list");
-            if (ft.kind == FCC_OVERLAP && (ft.nJ < 1 || ft.nJ > FCC_MAX_TYPES))
-                return fail(FCC_ERR_DIMENSION, "coupling tables must be square and equal-sized");
-        }
-        N = b->n;
-        if (N < 0) return fail(FCC_ERR_DIMENSION, "inconsistent body array lengths");
-        if (N > (1 << 27)) return fail(FCC_ERR_UNSUPPORTED, "at most 2^27 bodies per simulation");
-        int32_t maxtype = 0;
-        for (int64_t i = 0; i < N; ++i) {
-            if (b->type[i] > p->ntypes) return fail(FCC_ERR_ARGUMENT, "body type without BodyType entry");
-            if (b->type[i] < 1) return fail(FCC_ERR_ARGUMENT, "body type ids are 1-based");
-            maxtype = std::max(maxtype, b->type[i]);
-        }
-        for (int q = 0; q < p->nterms; ++q) {
-            const fcc_term& ft = p->terms[q];
-            if (ft.kind == FCC_OVERLAP && ft.nJ > 1 && ft.nJ < maxtype)
-                return fail(FCC_ERR_DIMENSION, "Overlap coupling table smaller than the number of body types");
-        }
-        for (int64_t i = 0; i < N; ++i) {  // check_parents, src/simulation.jl:108-118
-            int64_t pp = b->parent[i];
-            if (pp < 1 || pp > N)
-                return fail(FCC_ERR_ARGUMENT, "body " + std::to_string(i + 1) + " has parent " + std::to_string(pp) +
-                                                  " outside 1:" + std::to_string(N));
-            if (!p->types[b->type[i] - 1].parent_drag) continue;
-            if (pp == i + 1)
-                return fail(FCC_ERR_ARGUMENT, "body " + std::to_string(i + 1) + " has drag = :parent but is its own parent");
-            if (p->types[b->type[pp - 1] - 1].parent_drag)
-                return fail(FCC_ERR_ARGUMENT, "body " + std::to_string(i + 1) + " has drag = :parent, but so has its parent " +
-                                                  std::to_string(pp) + " (one level only)");
-        }
-        K = b->ncoef / 2;
-        nth = p->ntheta;
-        if (K + 1 < 2) return fail(FCC_ERR_ARGUMENT, "maxmode must be ≥ 2");
-        if (!(nth > 2 * (K + 1))) return fail(FCC_ERR_ARGUMENT, "nθ must exceed 2·maxmode");
-        nc = 2 * K + 1;
-        if (b->ncoef != nc) return fail(FCC_ERR_DIMENSION, "coefficient rows must be odd: [a₀; aₙ; bₙ]");
-        if (K > KM) return fail(FCC_ERR_UNSUPPORTED, "this build supports maxmode ≤ 10");
-        if (!(p->skin >= 0)) return fail(FCC_ERR_ARGUMENT, "skin must be non-negative");
-
+        SimSpec<T> sp;
+        FCC_TRY(make_spec(p, b, sp));
         // device and stream
         CUDA_TRY(cudaGetDevice(&device));
         CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
@@ -290,153 +478,24 @@ struct Engine final : EngineBase {
         CUDA_TRY(cudaEventCreate(&ev1));
         CUDA_TRY(cudaMallocHost(&st_h, sizeof(Status)));
 
-        // simulation descriptor (convert_precision: every parameter to T)
-        SimDesc<T>& s = desc;
-        s.Lx = (T)p->Lx;
-        s.Ly = (T)p->Ly;
-        s.invLx = T(1) / s.Lx;
-        s.invLy = T(1) / s.Ly;
-        s.dt = (T)p->dt;
-        s.skin = (T)p->skin;
-        s.crange = T(0);  // interaction_range of the built-in contact terms
-        s.nbrange = s.crange + s.skin;
-        s.dphi = (T)(2 * PI / nth);
-        R0_h.resize(N);
-        double maxR0 = 0;
-        for (int64_t i = 0; i < N; ++i) {
-            R0_h[i] = (T)b->R0[i];
-            maxR0 = std::max(maxR0, (double)R0_h[i]);
-        }
-        const double cutoff = 2 * maxR0 * (1 + SHAPE_BOUND) + 0.0 + p->skin;  // src/simulation.jl:90
-        auto ncells = [&](T L) {
-            int64_t n = (int64_t)std::floor((double)L / cutoff);
-            return (int)(n >= 3 ? n : 1);
-        };
-        ncx = ncells(s.Lx);
-        ncy = ncells(s.Ly);
-        if ((int64_t)ncx * ncy > (1 << 28)) return fail(FCC_ERR_UNSUPPORTED, "cell grid too large");
-        s.wx = s.Lx / (T)ncx;
-        s.wy = s.Ly / (T)ncy;
-        s.ncx = ncx;
-        s.ncy = ncy;
-        s.cell_off = 0;
-        s.ncells = ncx * ncy;
-        s.body_off = 0;
-        s.n = (int)N;
-        s.nth = nth;
-        s.K = K;
-        s.k0 = (uint32_t)(p->seed & 0xffffffffu);
-        s.k1 = (uint32_t)(p->seed >> 32);
-        s.ntypes = p->ntypes;
-        s.rewrap = (ncx < 3 || ncy < 3) ? 1 : 0;
-        for (int t = 0; t < p->ntypes; ++t) {
-            const fcc_body_type& bt = p->types[t];
-            s.v0[t] = (T)bt.v0;
-            s.Dr[t] = (T)bt.Dr;
-            s.Dt[t] = (T)bt.Dt;
-            s.mur[t] = (T)bt.mu_r;
-            s.muth[t] = (T)bt.mu_theta;
-            s.muab[t] = (T)bt.mu_ab;
-            s.parent_drag[t] = bt.parent_drag;
-        }
-        auto mask_of = [](const fcc_term& ft) {
-            if (ft.ntypes_on == 0) return 0xffffffffu;
-            uint32_t m = 0;
-            for (int u = 0; u < ft.ntypes_on; ++u)
-                if (ft.types_on[u] >= 1 && ft.types_on[u] <= FCC_MAX_TYPES) m |= 1u << (ft.types_on[u] - 1);
-            return m;
-        };
-        // contact couplings summed over terms in the reference's order g1 + (g2 + ...)
-        for (int r = 0; r < 2; ++r)
-            for (int a = 0; a < MT; ++a)
-                for (int c = 0; c < MT; ++c) s.cA[r][a][c] = T(0);
-        for (int a = 0; a < MT; ++a) s.cB[a] = T(0);
-        for (int q = p->nterms - 1; q >= 0; --q) {
-            const fcc_term& ft = p->terms[q];
-            const uint32_t mk = mask_of(ft);
-            if (ft.kind == FCC_OVERLAP) {
-                has_contact = true;
-                for (int a = 0; a < MT; ++a) {
-                    if (!((mk >> a) & 1u)) continue;
-                    for (int c = 0; c < MT; ++c) {
-                        const int ij = ft.nJ == 1 ? 0 : (a < ft.nJ && c < ft.nJ ? a + ft.nJ * c : -1);
-                        if (ij < 0) continue;
-                        s.cA[0][a][c] = (T)ft.J[ij] + s.cA[0][a][c];
-                        s.cA[1][a][c] = (T)ft.Jrel[ij] + s.cA[1][a][c];
-                    }
-                }
-            } else if (ft.kind == FCC_LINEAR_REPULSION) {
-                has_contact = true;
-                for (int a = 0; a < MT; ++a)
-                    if ((mk >> a) & 1u) s.cB[a] = (T)ft.a + s.cB[a];
-            }
-        }
-        s.nbt = 0;
-        s.nbd = 0;
-        for (int q = 0; q < p->nterms; ++q) {
-            const fcc_term& ft = p->terms[q];
-            if (ft.kind == FCC_TENSION || ft.kind == FCC_PERIMETER_ELASTICITY) {
-                const int u = s.nbt++;
-                s.bt_kind[u] = ft.kind == FCC_TENSION ? BT_TENSION : BT_PERIMETER;
-                s.bt_mask[u] = mask_of(ft);
-                s.bt_a[u] = (T)ft.a;
-                // l0 = p0 * sqrt(π) * R0 (src/energies/body_terms.jl:34)
-                s.bt_b[u] = ft.kind == FCC_TENSION ? T(0) : (T)ft.b * std::sqrt((T)PI);
-            } else if (ft.kind == FCC_HARMONIC_BOND) {
-                const int u = s.nbd++;
-                s.bd_mask[u] = mask_of(ft);
-                s.bd_k[u] = (T)ft.a;
-                s.bd_r0[u] = (T)ft.b;
-            }
-        }
-        s.has_contact = has_contact ? 1 : 0;
-        s.has_noise = 0;
-        for (int t = 0; t < p->ntypes; ++t)
-            if (p->types[t].Dr != 0 || p->types[t].Dt != 0) s.has_noise = 1;
-        split = false;
-        for (int64_t i = 0; i < N; ++i)
-            if (p->types[b->type[i] - 1].parent_drag) split = true;
-        s.has_parent_drag = split ? 1 : 0;
-
-        // children (src/bodies.jl:121-135) and bonds (src/energies/bonds.jl:52-71), global ids
-        type_h.assign(b->type, b->type + N);
-        parent_h.assign(b->parent, b->parent + N);
-        std::vector<int> chc(N, 0);
-        for (int64_t k = 0; k < N; ++k)
-            if (parent_h[k] != k + 1) chc[parent_h[k] - 1] += 1;
-        ccap = 1;
-        for (int64_t k = 0; k < N; ++k) ccap = std::max(ccap, chc[k]);
-        std::vector<int> chi((size_t)ccap * N, 0);
-        std::fill(chc.begin(), chc.end(), 0);
-        for (int64_t k = 0; k < N; ++k) {
-            const int pp = parent_h[k] - 1;
-            if (pp == k) continue;
-            chi[(size_t)pp * ccap + chc[pp]++] = (int)k;
-        }
-        std::vector<int> bdc(N, 0);
-        std::set<std::pair<int64_t, int64_t>> seen;
-        for (int64_t q = 0; q < p->nbonds; ++q) {
-            const int64_t i = p->bonds[2 * q], j = p->bonds[2 * q + 1];
-            if (!(1 <= i && i <= N && 1 <= j && j <= N))
-                return fail(FCC_ERR_ARGUMENT, "bond (" + std::to_string(i) + ", " + std::to_string(j) +
-                                                  ") refers to a body outside 1:" + std::to_string(N));
-            if (i == j)
-                return fail(FCC_ERR_ARGUMENT, "bond (" + std::to_string(i) + ", " + std::to_string(j) + ") connects a body to itself");
-            auto key = std::make_pair(std::min(i, j), std::max(i, j));
-            if (seen.count(key)) return fail(FCC_ERR_ARGUMENT, "duplicate bond (" + std::to_string(i) + ", " + std::to_string(j) + ")");
-            seen.insert(key);
-            bdc[i - 1] += 1;
-            bdc[j - 1] += 1;
-        }
-        bcap = 1;
-        for (int64_t k = 0; k < N; ++k) bcap = std::max(bcap, bdc[k]);
-        std::vector<int> bdi((size_t)bcap * N, 0);
-        std::fill(bdc.begin(), bdc.end(), 0);
-        for (int64_t q = 0; q < p->nbonds; ++q) {
-            const int64_t i = p->bonds[2 * q] - 1, j = p->bonds[2 * q + 1] - 1;
-            bdi[(size_t)i * bcap + bdc[i]++] = (int)j;
-            bdi[(size_t)j * bcap + bdc[j]++] = (int)i;
-        }
+        N = sp.N;
+        K = sp.K;
+        nc = sp.nc;
+        nth = sp.nth;
+        ncx = sp.ncx;
+        ncy = sp.ncy;
+        has_contact = sp.has_contact;
+        split = sp.split;
+        desc = sp.desc;
+        type_h = std::move(sp.type);
+        parent_h = std::move(sp.parent);
+        R0_h = std::move(sp.R0);
+        ccap = sp.ccap;
+        bcap = sp.bcap;
+        const std::vector<int>& chi = sp.chi;
+        const std::vector<int>& chc = sp.chc;
+        const std::vector<int>& bdi = sp.bdi;
+        const std::vector<int>& bdc = sp.bdc;
 
         // device buffers
         cap = p->nl_capacity > 0 ? p->nl_capacity : 32;
@@ -560,9 +619,9 @@ struct Engine final : EngineBase {
         const DevPtrs<T> d = ptrs();
         if (N > 0) {
             const int grid = (int)((N + 255) / 256);
-            k_init<T><<<grid, 256, 0, stream>>>(d, par(), bx.p, by.p, bth.p, bc.p);
+            k_init<T><<<grid, 256, 0, stream>>>(d, par(), 0, (int)N, bx.p, by.p, bth.p, bc.p);
             CUDA_TRY(cudaGetLastError());
-            k_set_w<T><<<grid, 256, 0, stream>>>(d, par(), bw.p);
+            k_set_w<T><<<grid, 256, 0, stream>>>(d, par(), 0, (int)N, bw.p);
             CUDA_TRY(cudaGetLastError());
         }
         // list invalid: the next step (or update_neighbors!) rebuilds
@@ -923,7 +982,7 @@ struct Engine final : EngineBase {
         if (N > 0) {
             DBuf<double> buf;
             FCC_TRY(buf.alloc(3 * (size_t)N, stream));
-            k_observables<T><<<(int)((N + 127) / 128), 128, 0, stream>>>(ptrs(), par(), buf.p);
+            k_observables<T><<<(int)((N + 127) / 128), 128, 0, stream>>>(ptrs(), par(), 0, (int)N, buf.p);
             CUDA_TRY(cudaGetLastError());
             CUDA_TRY(cudaMemcpyAsync(v.data(), buf.p, v.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
             FCC_TRY(sync_stream());
@@ -1079,6 +1138,7 @@ fcc_status build_neighbors_t(int64_t n, const double* x, const double* y, const 
 }  // namespace
 
 #include "fcc_noalloc.cu"
+#include "fcc_pool.cu"
 
 struct fcc_sim {
     std::unique_ptr<EngineBase> impl;

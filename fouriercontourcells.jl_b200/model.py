@@ -36,6 +36,10 @@ class DeviceError(RuntimeError):
     """CUDA or device-side failure reported by the native library."""
 
 
+class PoolFull(RuntimeError):
+    """A pool has no free slot, bodies or grid cells for a simulation now."""
+
+
 # --------------------------------------------------------------------- types
 @dataclass(frozen=True)
 class BodyType:

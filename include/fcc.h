@@ -46,7 +46,8 @@ enum {
     FCC_ERR_CUDA = 3,        /* CUDA runtime error (message has the CUDA text) */
     FCC_ERR_UNSUPPORTED = 4, /* valid model outside this build's kernels */
     FCC_ERR_DEVICE = 5,      /* device-side error status (e.g. non-finite state) */
-    FCC_ERR_NOMEM = 6        /* device allocation failed */
+    FCC_ERR_NOMEM = 6,       /* device allocation failed */
+    FCC_ERR_FULL = 7         /* pool: no room for this simulation until others leave */
 };
 
 /* Energy term kinds (src/energies/body_terms.jl, contact.jl, bonds.jl). */
@@ -242,6 +243,78 @@ fcc_status fcc_build_neighbors_noalloc(int32_t precision, int64_t n, const void*
  * stream): elapsed milliseconds, launches of this library's kernels, and
  * steps executed. */
 fcc_status fcc_last_timing(fcc_sim* sim, double* ms, int64_t* launches, int64_t* steps);
+
+/* ------------------------------------------------------------------ pool --
+ * Many simulations packed into one engine: their bodies, grid cells and
+ * neighbour lists share one device arena, and one persistent step kernel
+ * launch advances all of them.  The reference runs concurrent simulations as
+ * independent `Simulation`s on separate tasks/streams (README.md:255-262);
+ * this is the batched form of that, for monolayers of uneven N (batching) and
+ * for a request loop that admits and retires simulations while others run
+ * (serving).  Each simulation keeps the semantics of fcc_create/fcc_run: its
+ * own box, types, terms, dt, seed and Philox stream, its own neighbour-list
+ * rebuilds, and results equal to running it alone with the same kernel
+ * variant (fcc_pool_variant) — bit for bit.
+ *
+ * A pool is sized once (fcc_pool_bytes gives its device footprint, so a caller
+ * sizes it from an HBM budget).  Every simulation's bodies start at a multiple
+ * of FCC_POOL_ALIGN in the arena; the arena is kept dense (retired
+ * simulations are compacted away before the next run). */
+#define FCC_POOL_ALIGN 8
+
+typedef struct fcc_pool fcc_pool;
+
+typedef struct {
+    int32_t precision;    /* 32 or 64, for every simulation of the pool */
+    int32_t ntheta;       /* contour nodes, for every simulation of the pool */
+    int64_t max_bodies;   /* arena capacity in bodies (each simulation padded to FCC_POOL_ALIGN) */
+    int64_t max_cells;    /* arena capacity in grid cells */
+    int32_t max_sims;     /* simulation slots */
+    int32_t nl_capacity;  /* initial neighbours per body (0: 32); grows on overflow */
+    int32_t max_children; /* children per body (0: 1) */
+    int32_t max_bonds;    /* bonds per body (0: 1) */
+} fcc_pool_params;
+
+/* Device bytes a pool of these limits holds (both arena copies, lists, slots). */
+fcc_status fcc_pool_bytes(const fcc_pool_params* params, int64_t* bytes);
+fcc_status fcc_pool_create(const fcc_pool_params* params, fcc_pool** out);
+fcc_status fcc_pool_destroy(fcc_pool* pool);
+
+/* Admit one simulation (the arguments of fcc_create; params->precision and
+ * params->ntheta must equal the pool's) that will run `horizon` steps.
+ * FCC_ERR_FULL: no free slot, bodies or cells now (nothing changed). */
+fcc_status fcc_pool_add(fcc_pool* pool, const fcc_params* params, const fcc_bodies_host* bodies, int64_t horizon,
+                        int32_t* slot);
+/* Retire a simulation; its room is reclaimed before the next run or add. */
+fcc_status fcc_pool_remove(fcc_pool* pool, int32_t slot);
+
+/* Advance every admitted simulation by min(n, horizon - steps done) steps in
+ * persistent multi-step launches of the packed step kernel. */
+fcc_status fcc_pool_run(fcc_pool* pool, int64_t n);
+
+/* Steps done and horizon of a slot; *active = 0 for a free slot. */
+fcc_status fcc_pool_slot(fcc_pool* pool, int32_t slot, int32_t* active, int64_t* steps, int64_t* horizon);
+/* Bodies, cells and slots in use, and the capacities. */
+fcc_status fcc_pool_usage(fcc_pool* pool, int64_t* bodies, int64_t* cells, int32_t* sims, int64_t* max_bodies,
+                          int64_t* max_cells, int32_t* max_sims);
+
+/* fcc_get_state / fcc_shape_index (perimeters: which = 0, areas: 1, shape
+ * index: 2) and sim.neighbors.builds of one slot. */
+fcc_status fcc_pool_get_state(fcc_pool* pool, int32_t slot, fcc_bodies_host* out, int64_t* clock, double* t,
+                              int64_t* step);
+fcc_status fcc_pool_observable(fcc_pool* pool, int32_t slot, int32_t which, int32_t type, double* out,
+                               int64_t* count);
+fcc_status fcc_pool_builds(fcc_pool* pool, int32_t slot, int64_t* builds);
+
+/* Launch configuration: kernel variant (index into the library's table; -1:
+ * the autotuned or default choice) and steps per launch (0: 512). */
+fcc_status fcc_pool_config(fcc_pool* pool, int32_t variant, int32_t steps_per_launch);
+fcc_status fcc_pool_variant(fcc_pool* pool, int32_t* variant, int32_t* lanes, int32_t* slots, int32_t* block,
+                            int32_t* min_blocks, int32_t* grid);
+
+/* Device timing of the last fcc_pool_run: milliseconds, launches, and
+ * body-steps executed (summed over simulations). */
+fcc_status fcc_pool_last_timing(fcc_pool* pool, double* ms, int64_t* launches, int64_t* body_steps);
 
 /* Message of the last error on this thread. */
 const char* fcc_last_error(void);

@@ -37,8 +37,8 @@ def test_library_exports_every_declared_symbol():
 def test_oracle_exports_mirror():
     lib = oracle.library()
     for n in declared_functions():
-        if n in ("fcc_run", "fcc_last_timing", "fcc_version", "fcc_build_neighbors_noalloc"):
-            continue
+        if n in ("fcc_run", "fcc_last_timing", "fcc_version", "fcc_build_neighbors_noalloc") or n.startswith("fcc_pool_"):
+            continue  # device-only entry points (launch timing, caller device arrays, packed pools)
         assert hasattr(lib, "fcco_" + n[4:]), n
 
 
@@ -46,9 +46,9 @@ def test_struct_layouts_match_header():
     """Sizes of the ctypes mirror against a C compile of fcc.h."""
     import subprocess
     import tempfile
-    src = '#include <stdio.h>\n#include "fcc.h"\nint main(){printf("%zu %zu %zu %zu %zu %zu %zu\\n",' \
+    src = '#include <stdio.h>\n#include "fcc.h"\nint main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n",' \
           'sizeof(fcc_term),sizeof(fcc_body_type),sizeof(fcc_params),sizeof(fcc_bodies_host),' \
-          'sizeof(fcc_gradients_host),sizeof(fcc_geometry_host),sizeof(fcc_neighbors_host));}'
+          'sizeof(fcc_gradients_host),sizeof(fcc_geometry_host),sizeof(fcc_neighbors_host),sizeof(fcc_pool_params));}'
     with tempfile.TemporaryDirectory() as d:
         c = os.path.join(d, "s.c")
         open(c, "w").write(src)
@@ -57,7 +57,8 @@ def test_struct_layouts_match_header():
         sizes = list(map(int, subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()))
     a = fcc.abi
     assert sizes == [C.sizeof(a.FccTerm), C.sizeof(a.FccBodyType), C.sizeof(a.FccParams), C.sizeof(a.FccBodiesHost),
-                     C.sizeof(a.FccGradientsHost), C.sizeof(a.FccGeometryHost), C.sizeof(a.FccNeighborsHost)]
+                     C.sizeof(a.FccGradientsHost), C.sizeof(a.FccGeometryHost), C.sizeof(a.FccNeighborsHost),
+                     C.sizeof(a.FccPoolParams)]
 
 
 def test_product_fails_loudly_without_library(monkeypatch):
@@ -112,3 +113,22 @@ def test_initial_conditions():
     c = fcc.vcat(fcc.Bodies.new([1.0, 2.0], [1.0, 2.0], np.zeros(2), np.zeros((11, 2)), np.ones(2), parent=[1, 1]),
                  fcc.Bodies.new([3.0, 4.0], [3.0, 4.0], np.zeros(2), np.zeros((11, 2)), np.ones(2), type=2, parent=[2, 2]))
     assert list(c.parent) == [1, 1, 4, 4] and list(c.type) == [1, 1, 2, 2]
+
+
+def test_pool_host_helpers():
+    """Arena padding and grid-cell counts the pool's admission uses."""
+    from conftest import fcc as f
+    assert [f.pool.padded(n) for n in (0, 1, 8, 9, 30)] == [0, 8, 8, 16, 32]
+    bodies, box = f.polydisperse_monolayer(128, 128, packing=0.95, maxmode=10, seed=1234)
+    # cutoff 2 * 1.2 * (1 + sqrt(2/3)) + 0.3 = 4.66: a 53 x 46 grid
+    assert f.pool.grid_cells(box, bodies.R0, T=np.float32) == 53 * 46
+
+
+def test_pool_device_bytes_without_gpu():
+    """The footprint query needs no device (admission by HBM budget)."""
+    b1 = fcc.Pool.device_bytes(np.float32, 40, 1 << 20, 1 << 18, 256)
+    b2 = fcc.Pool.device_bytes(np.float32, 40, 2 << 20, 1 << 18, 256)
+    b64 = fcc.Pool.device_bytes(np.float64, 40, 1 << 20, 1 << 18, 256)
+    assert 0 < b1 < b2 < 2 * b1 + (1 << 22) and b64 > b1
+    per_body = (b2 - b1) / (1 << 20)
+    assert 400 < per_body < 2000
