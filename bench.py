@@ -229,6 +229,112 @@ def batched_leg(fcc, steps=2000, warm=3, count=256):
             "bitwise_equal_to_plain": f"{equal}/{count}"}
 
 
+# ------------------------------------------------------------ accuracy
+def force_error(fcc, oracle, bodies, box, kw, near_tie=3e-6):
+    """FP32 forces of the CUDA path against the FP64 oracle on the same
+    (FP32-representable) state: max |error| / max |oracle value| per field,
+    bodies with an Overlap near-tie |d| < 3e-6 excluded (the Heaviside
+    g = J H(d) may flip there in FP32) and counted."""
+    b = bodies.copy()
+    for f in ("x", "y", "θ", "coef", "R0"):
+        setattr(b, f, np.asarray(getattr(b, f), dtype=np.float32).astype(np.float64))
+    g = fcc.Simulation(b, box, T=np.float32, **kw)
+    g.refresh()  # neighbour lists of this state, then compute_gradients!
+    o = oracle.OracleSimulation(b, box, T=np.float64, **kw)
+    o.refresh()
+    keep = ~(o.contact_counters()[2] < near_tie)
+    out = {}
+    for f in ("gx", "gy", "gθ", "gcoef", "Ebody"):
+        a, r = np.asarray(getattr(g.grad, f), float), np.asarray(getattr(o.grad, f), float)
+        scale = max(float(np.abs(r).max()), 1e-300)
+        out[f] = float(np.abs(a[..., keep] - r[..., keep]).max() / scale) if keep.any() else 0.0
+    g.close()
+    return {"max_rel": max(out.values()), "fields": out, "excluded_near_ties": float(1 - keep.mean()),
+            "definition": "max |F32 - F64| / max |F64| per field on the same state, near-ties |d| < 3e-6 excluded"}
+
+
+# ------------------------------------------------------------ serving
+SERVE_WORKLOAD = ("Poisson stream (lambda = 20 req/s) of requests: N log-uniform on [256, 65536] (square-ish "
+                  "hexagonal packings at 0.95, R0 ~ N(1, 0.1) clipped to [0.8, 1.2]), horizon U[1000, 50000] "
+                  "steps, v0 U[0.02, 0.2], eta U[0.001, 0.1], Dr U[0.005, 0.05], Tension(eta) + Overlap(1.0), "
+                  "mu_ab 0.1, dt 0.005, per-request Philox seed, FP32 bulk with FP64 a0/projection")
+
+
+def serve_stream(count=2000, rate=20.0, seed=77):
+    """Specs of the serving stream (bodies are made on demand)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(count):
+        t += float(rng.exponential(1.0 / rate))
+        n_t = math.exp(rng.uniform(math.log(256), math.log(65536)))
+        ny = max(2, 2 * round(math.sqrt(2 * n_t / math.sqrt(3)) / 2))
+        nx = max(1, round(n_t / ny))
+        out.append(dict(id=i, arrival=t, nx=nx, ny=ny, horizon=int(rng.integers(1000, 50001)),
+                        v0=float(rng.uniform(0.02, 0.2)), eta=float(rng.uniform(0.001, 0.1)),
+                        Dr=float(rng.uniform(0.005, 0.05)), seed=int(rng.integers(1, 2**31 - 1))))
+    return out
+
+
+def make_request(fcc, sp):
+    bodies, box = fcc.polydisperse_monolayer(sp["nx"], sp["ny"], packing=0.95, maxmode=10, seed=sp["seed"])
+    kw = dict(types=(fcc.BodyType(v0=sp["v0"], Dr=sp["Dr"], μab=0.1),),
+              energies=(fcc.Tension(sp["eta"]), fcc.Overlap(1.0)), dt=0.005, seed=sp["seed"])
+    return fcc.Request(bodies, box, kw, sp["horizon"], sp["arrival"], sp["id"])
+
+
+def serving_leg(fcc, oracle, work=1.5e10, pool_bodies=1 << 19):
+    """The first requests of the serving stream (up to `work` body-steps),
+    served by continuous batching on one pool sized from an HBM budget, then
+    the same requests run one at a time (the plain loop)."""
+    import torch
+    stream = serve_stream()
+    offered = 20.0 * float(np.mean([sp["nx"] * sp["ny"] * sp["horizon"] for sp in stream]))
+    sample, acc = [], 0.0
+    for sp in stream:
+        w = sp["nx"] * sp["ny"] * sp["horizon"]
+        if sample and acc + w > work:
+            break
+        sample.append(sp)
+        acc += w
+    reqs = [make_request(fcc, sp) for sp in sample]
+    budget = fcc.Pool.device_bytes(np.float32, 40, pool_bodies, pool_bodies // 4, 256)
+    pool = fcc.Pool.for_budget(budget, T=np.float32, max_sims=256)
+    srv = fcc.Server(pool, chunk=512)
+    torch.cuda.synchronize()
+    res = srv.serve(reqs)
+    served = fcc.serving.summary(res)
+    by_id = {r.id: r for r in res}
+    # the plain loop: each request alone, in arrival order
+    durations, equal = [], 0
+    for r in reqs:
+        t0 = time.perf_counter()
+        sim = fcc.Simulation(r.bodies, r.box, T=np.float32, **r.kw)
+        sim.run(r.horizon)
+        b = sim.bodies
+        durations.append(time.perf_counter() - t0)
+        c = by_id[r.id].bodies
+        equal += int(all(np.array_equal(getattr(b, f), getattr(c, f)) for f in ("x", "y", "θ", "coef", "imgx")))
+        sim.close()
+    lat = fcc.serving.sequential_latencies([r.arrival for r in reqs], durations)
+    plain_span = max(a + l for a, l in zip((r.arrival for r in reqs), lat)) - min(r.arrival for r in reqs)
+    plain = {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+             "body_steps_per_s": served["body_steps"] / plain_span}
+    # 1% audited sample (at least one request): force error of the served result
+    audit = [r for r in reqs if r.id % 100 == 0] or reqs[:1]
+    errs = {r.id: force_error(fcc, oracle, by_id[r.id].bodies, r.box, r.kw)["max_rel"] for r in audit}
+    u = pool.usage()
+    pool.close()
+    return {"workload": SERVE_WORKLOAD,
+            "sample": f"the first {len(reqs)} requests of the seeded 2000-request stream ({acc:.3g} body-steps)",
+            "offered_body_steps_per_s": offered,
+            "pool": {"hbm_budget_bytes": budget, "max_bodies": u["max_bodies"], "max_sims": u["max_sims"]},
+            "served": served, "plain": plain,
+            "served_over_plain": served["body_steps_per_s"] / plain["body_steps_per_s"],
+            "chunks": srv.chunks, "bitwise_equal_to_alone": f"{equal}/{len(reqs)}",
+            "audit_force_error_vs_fp64": errs}
+
+
 # ------------------------------------------------------------------ arms
 def cpu_baseline(fcc, oracle, budget_s=15.0, max_steps=200):
     """The oracle (FP64, OpenMP on all host cores) on the same workload,
@@ -365,6 +471,8 @@ def gpu_arm(args):
         achieved_tf = flops_b * N * steps_per_launch / (launch_ms * 1e-3) / 1e12
         cpu, _ = cpu_baseline(fcc, oracle)
         batched = batched_leg(fcc) if not args.skip_batched else None
+        served = serving_leg(fcc, oracle, work=args.serve_work) if args.serve_work > 0 else None
+        ferr = force_error(fcc, oracle, out, box, kw)
         line = {
             "metric": METRIC, "value": value, "unit": "body-steps/s", "n_gpus": world, "steps": steps,
             "warmup": args.warmup, "ms_per_step": ms_max / steps, "higher_is_better": True, "scaling": "weak",
@@ -387,7 +495,9 @@ def gpu_arm(args):
             "gpu_launches": launches * world,
             "clocks": cs,
             "builds": sim.builds,
+            "err_vs_fp64": ferr,
             "batched": batched,
+            "serving": served,
         }
         print(json.dumps(line), flush=True)
     if dist:
@@ -402,6 +512,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=200)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--skip-batched", action="store_true", help="leave out the batching leg")
+    ap.add_argument("--serve-work", type=float, default=1.5e10,
+                    help="body-steps of the serving sample (0: leave out the serving leg)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

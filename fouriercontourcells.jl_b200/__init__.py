@@ -22,9 +22,10 @@ from .simulation import (Simulation, NativeSimulation, native_library, step, run
                          unwrapped_positions, contours, protrusion, Gradients, Geometry, NeighborInfo)
 from .ops import philox_noise, build_neighbors
 from .pool import Pool
+from .serving import Request, Result, Server
 
 __all__ = [
-    "ArgumentError", "DimensionMismatch", "DeviceError", "PoolFull", "Pool", "BodyType", "EnergyTerm", "BodyTerm", "ContactTerm",
+    "ArgumentError", "DimensionMismatch", "DeviceError", "PoolFull", "Pool", "Request", "Result", "Server", "BodyType", "EnergyTerm", "BodyTerm", "ContactTerm",
     "BondTerm", "Tension", "PerimeterElasticity", "Overlap", "LinearRepulsion", "HarmonicBond", "OnTypes",
     "Bodies", "PeriodicBox", "vcat", "nbodies", "hexagonal_monolayer", "with_nuclei", "parent_bonds",
     "polydisperse_monolayer", "minimum_image", "wrap", "Simulation", "NativeSimulation", "native_library", "step",

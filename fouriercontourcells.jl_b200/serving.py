@@ -1,0 +1,139 @@
+"""Serving: a request loop that keeps simulations resident in a ``Pool``.
+
+Continuous batching for simulation requests (no counterpart in the
+reference, whose callers run one ``Simulation`` per task): requests arrive
+over time with their own bodies, parameters, seed and horizon; the loop
+admits them, in arrival order, whenever the pool has a free slot and room for
+their bodies and grid cells (the pool is sized from an HBM budget,
+``Pool.for_budget``); all admitted simulations advance together in the packed
+step kernel, chunk by chunk; a simulation that reaches its horizon is read
+back (state and shape index) and retired at the end of that chunk, which
+frees its room for the requests still waiting.  Each result equals the one of
+the same request run alone with the same kernel variant, bit for bit.
+"""
+
+from __future__ import annotations
+
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .model import ArgumentError, Bodies, PeriodicBox
+from .pool import grid_cells, padded
+
+
+@dataclass
+class Request:
+    """One simulation request: ``Simulation(bodies, box; kw...)`` run for ``horizon`` steps."""
+    bodies: Bodies
+    box: PeriodicBox
+    kw: dict
+    horizon: int
+    arrival: float = 0.0  # seconds after the stream starts
+    id: int = 0
+
+    @property
+    def work(self) -> int:
+        return self.bodies.n * self.horizon
+
+
+@dataclass
+class Result:
+    id: int
+    n: int
+    horizon: int
+    arrival: float
+    admitted: float
+    finished: float
+    bodies: Bodies = field(repr=False)
+    shape_index_mean: float = float("nan")
+
+    @property
+    def latency(self) -> float:
+        """Time to result: arrival to the result on the host."""
+        return self.finished - self.arrival
+
+
+class Server:
+    """Continuous-batching loop over a pool.
+
+    ``chunk`` caps the steps between two admission/retirement points; the loop
+    shortens a chunk to the fewest steps any admitted simulation has left, so a
+    finished simulation leaves (and frees its room) at once."""
+
+    def __init__(self, pool, chunk=512, min_chunk=32, T=np.float32, clock=time.perf_counter, sleep=time.sleep):
+        self.pool = pool
+        self.chunk = int(chunk)
+        self.min_chunk = int(min_chunk)
+        self.T = T
+        self.clock = clock
+        self.sleep = sleep
+        self.chunks = 0
+
+    def _fits_empty(self, r: Request) -> bool:
+        u = self.pool.usage()
+        cells = grid_cells(r.box, r.bodies.R0, r.kw.get("skin", 0.3), self.T)
+        return padded(r.bodies.n) <= u["max_bodies"] and cells <= u["max_cells"]
+
+    def serve(self, requests, on_result=None):
+        """Run the stream; returns the results in completion order."""
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        for r in pending:
+            if not self._fits_empty(r):
+                raise ArgumentError(f"request {r.id} ({r.bodies.n} bodies) does not fit in an empty pool")
+        waiting = deque()
+        active = {}  # slot -> (request, admitted)
+        results = []
+        t0 = self.clock()
+        now = lambda: self.clock() - t0
+        while pending or waiting or active:
+            t = now()
+            while pending and pending[0].arrival <= t:
+                waiting.append(pending.popleft())
+            while waiting:  # admission in arrival order, as slots and memory free up
+                r = waiting[0]
+                slot = self.pool.try_add(r.bodies, r.box, horizon=r.horizon, **r.kw)
+                if slot is None:
+                    break
+                waiting.popleft()
+                active[slot] = (r, now())
+            if not active:
+                if pending:
+                    self.sleep(max(0.0, pending[0].arrival - now()))
+                continue
+            left = min(r.horizon - self.pool.slot(s)[1] for s, (r, _) in active.items())
+            self.pool.run(max(min(self.chunk, left), min(self.min_chunk, self.chunk)))
+            self.chunks += 1
+            for s in [s for s in active if self.pool.done(s)]:
+                r, adm = active.pop(s)
+                b = self.pool.bodies(s)
+                si = self.pool.shape_index(s)
+                self.pool.remove(s)
+                res = Result(r.id, r.bodies.n, r.horizon, r.arrival, adm, now(), b,
+                             float(np.mean(si)) if len(si) else float("nan"))
+                results.append(res)
+                if on_result:
+                    on_result(res)
+        return results
+
+
+def summary(results, makespan=None):
+    """p50/p99 time to result and body-steps/s of a served stream."""
+    lat = np.array([r.latency for r in results])
+    work = sum(r.n * r.horizon for r in results)
+    span = makespan if makespan is not None else max(r.finished for r in results) - min(r.arrival for r in results)
+    return {"requests": len(results), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()), "body_steps": int(work), "makespan_s": float(span),
+            "body_steps_per_s": work / span if span > 0 else float("nan")}
+
+
+def sequential_latencies(arrivals, durations):
+    """Times to result of a loop that runs requests one at a time in arrival
+    order (start = max(arrival, previous finish))."""
+    t, out = 0.0, []
+    for a, d in zip(arrivals, durations):
+        t = max(t, a) + d
+        out.append(t - a)
+    return np.array(out)

@@ -1,0 +1,129 @@
+"""Host logic of the serving loop (continuous batching) on CPU, with a fake
+pool and a fake clock: admission in arrival order as slots and memory free
+up, admission while other requests are running, retirement at the end of
+the chunk a request finishes in, rejection of requests that never fit, and
+the p50/p99 statistics.  The GPU pool itself is covered by test_gpu_pool.py
+and test_gpu_serving.py."""
+
+import numpy as np
+import pytest
+
+from conftest import fcc
+
+serving = fcc.serving
+
+
+class FakeClock:
+    def __init__(self):
+        self.t = 0.0
+
+    def __call__(self):
+        return self.t
+
+    def sleep(self, dt):
+        self.t += max(0.0, dt)
+
+
+class FakePool:
+    """The Pool interface the server uses; a step of all admitted bodies
+    costs bodies / rate seconds of the fake clock."""
+
+    def __init__(self, clock, max_bodies=256, max_cells=10_000, max_sims=4, rate=1e6):
+        self.clock, self.rate = clock, rate
+        self.cap = dict(max_bodies=max_bodies, max_cells=max_cells, max_sims=max_sims)
+        self.sims, self.next, self.log = {}, 0, []
+
+    def usage(self):
+        return dict(bodies=sum(serving.padded(s["n"]) for s in self.sims.values()),
+                    cells=sum(s["cells"] for s in self.sims.values()), sims=len(self.sims), **self.cap)
+
+    def try_add(self, bodies, box, horizon, **kw):
+        u = self.usage()
+        cells = serving.grid_cells(box, bodies.R0, kw.get("skin", 0.3), np.float32)
+        if (u["sims"] >= u["max_sims"] or u["bodies"] + serving.padded(bodies.n) > u["max_bodies"]
+                or u["cells"] + cells > u["max_cells"]):
+            return None
+        slot = min(set(range(self.cap["max_sims"])) - set(self.sims))
+        self.sims[slot] = dict(n=bodies.n, cells=cells, horizon=horizon, steps=0, seed=kw["seed"], bodies=bodies)
+        self.log.append(("add", kw["seed"], self.clock.t))
+        return slot
+
+    def run(self, n):
+        self.log.append(("run", n, sorted(s["seed"] for s in self.sims.values())))
+        busy = sum(s["n"] for s in self.sims.values() if s["steps"] < s["horizon"])
+        for s in self.sims.values():
+            s["steps"] += min(n, s["horizon"] - s["steps"])
+        self.clock.t += n * busy / self.rate
+
+    def slot(self, s):
+        x = self.sims[s]
+        return True, x["steps"], x["horizon"]
+
+    def done(self, s):
+        x = self.sims[s]
+        return x["steps"] >= x["horizon"]
+
+    def bodies(self, s):
+        return self.sims[s]["bodies"]
+
+    def shape_index(self, s):
+        return np.full(self.sims[s]["n"], 3.6)
+
+    def remove(self, s):
+        self.log.append(("remove", self.sims[s]["seed"], self.clock.t))
+        del self.sims[s]
+
+
+def req(i, nx, ny, horizon, arrival):
+    b, box = fcc.hexagonal_monolayer(nx, ny, packing=0.95, maxmode=10, rng=i)
+    return fcc.Request(b, box, dict(types=(fcc.BodyType(),), energies=(fcc.Tension(0.01),), seed=i), horizon,
+                       arrival, i)
+
+
+def test_continuous_batching_admits_while_others_run():
+    clk = FakeClock()
+    pool = FakePool(clk, max_bodies=160, max_sims=4)
+    # r0: 96 bodies, long; r1: 48 bodies, short; r2 arrives while both run and
+    # fits only once r1 has left; r3 arrives later and fits beside r0 and r2
+    reqs = [req(0, 8, 12, 5000, 0.0), req(1, 8, 6, 300, 0.0), req(2, 8, 6, 400, 0.01), req(3, 2, 4, 200, 0.4)]
+    srv = fcc.Server(pool, chunk=256, min_chunk=1, clock=clk, sleep=clk.sleep)
+    res = srv.serve(reqs)
+    order = [r.id for r in res]
+    assert order.index(1) < order.index(2) < order.index(0)
+    adds = [e for e in pool.log if e[0] == "add"]
+    rem1 = next(e for e in pool.log if e[0] == "remove" and e[1] == 1)
+    add2 = next(e for e in adds if e[1] == 2)
+    assert add2[2] == rem1[2]            # r2 enters at the boundary r1 leaves
+    runs_with_0_and_2 = [e for e in pool.log if e[0] == "run" and 0 in e[2] and 2 in e[2]]
+    assert runs_with_0_and_2             # and shares the device with r0 (continuous batching)
+    # the chunk is cut to the fewest remaining steps: r1 leaves after exactly 300 steps
+    first_runs = [e[1] for e in pool.log if e[0] == "run"][:2]
+    assert first_runs == [256, 44]
+    assert all(r.latency >= 0 and r.admitted >= r.arrival for r in res)
+
+
+def test_fifo_admission_without_overtaking():
+    clk = FakeClock()
+    pool = FakePool(clk, max_bodies=128, max_sims=8)
+    reqs = [req(0, 8, 12, 1000, 0.0), req(1, 8, 8, 100, 0.01), req(2, 2, 2, 100, 0.02)]
+    fcc.Server(pool, chunk=128, clock=clk, sleep=clk.sleep).serve(reqs)
+    adds = [e[1] for e in pool.log if e[0] == "add"]
+    assert adds == [0, 1, 2]  # r2 would fit beside r0 but waits behind r1
+
+
+def test_idle_server_sleeps_until_arrival_and_rejects_oversized():
+    clk = FakeClock()
+    pool = FakePool(clk, max_bodies=64, max_sims=2)
+    res = fcc.Server(pool, clock=clk, sleep=clk.sleep).serve([req(0, 4, 4, 10, 5.0)])
+    assert res[0].admitted >= 5.0 and res[0].arrival == 5.0
+    with pytest.raises(fcc.ArgumentError):
+        fcc.Server(FakePool(FakeClock(), max_bodies=64), clock=clk, sleep=clk.sleep).serve([req(1, 10, 10, 10, 0)])
+
+
+def test_summary_and_sequential_latencies():
+    rs = [serving.Result(i, 10, 100, 0.1 * i, 0.1 * i, 0.1 * i + 1.0 + (i == 9) * 9, None) for i in range(10)]
+    s = serving.summary(rs)
+    assert s["requests"] == 10 and s["p50_s"] == pytest.approx(1.0) and s["p99_s"] > 9
+    assert s["body_steps"] == 10_000
+    lat = serving.sequential_latencies([0.0, 0.0, 5.0], [1.0, 2.0, 1.0])
+    assert np.allclose(lat, [1.0, 3.0, 1.0])
