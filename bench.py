@@ -470,7 +470,7 @@ def gpu_arm(args):
         fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
         achieved_tf = flops_b * N * steps_per_launch / (launch_ms * 1e-3) / 1e12
         cpu, _ = cpu_baseline(fcc, oracle)
-        batched = batched_leg(fcc) if not args.skip_batched else None
+        batched = batched_leg(fcc, steps=args.batch_steps) if not args.skip_batched else None
         served = serving_leg(fcc, oracle, work=args.serve_work) if args.serve_work > 0 else None
         ferr = force_error(fcc, oracle, out, box, kw)
         line = {
@@ -514,9 +514,19 @@ def main():
     ap.add_argument("--skip-batched", action="store_true", help="leave out the batching leg")
     ap.add_argument("--serve-work", type=float, default=1.5e10,
                     help="body-steps of the serving sample (0: leave out the serving leg)")
+    ap.add_argument("--batch-steps", type=int, default=2000, help="steps of the batching leg")
+    ap.add_argument("--only", choices=["batched", "serving"],
+                    help="run one leg alone and print its JSON (profiling; not the bench line)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.only:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        fcc = load_package()
+        out = batched_leg(fcc, steps=args.batch_steps) if args.only == "batched" else \
+            serving_leg(fcc, load_oracle(), work=args.serve_work)
+        print(json.dumps({"leg": args.only, **out}, default=str), flush=True)
     else:
         gpu_arm(args)
 
