@@ -197,6 +197,7 @@ def batched_leg(fcc, steps=2000, warm=3, count=256):
     pool = fcc.Pool(T=np.float32, max_bodies=sum(fcc.pool.padded(b.n) for b, _, _ in members),
                     max_cells=cells, max_sims=count)
     slots = [pool.add(b, box, horizon=warm + steps, **kw) for b, box, kw in members]
+    tuned = pool.tune(64)  # launch shape for this size bucket (snapshot restored)
     pool.run(warm)
     flush_l2()
     torch.cuda.synchronize()
@@ -205,6 +206,8 @@ def batched_leg(fcc, steps=2000, warm=3, count=256):
     wall_b = time.perf_counter() - t0
     ms_b, launches_b, bsteps = pool.last_timing()
     var = pool.variant()
+    var["autotuned"] = {"variant": tuned[0], "us_per_step": tuned[1]}
+    var["graph"] = dict(zip(("active", "replays"), pool.graph()))
     # plain loop
     ms_p, wall_p, equal = 0.0, 0.0, 0
     for (b, box, kw), slot in zip(members, slots):

@@ -200,6 +200,8 @@ struct PoolBase {
     virtual fcc_status config(int32_t variant, int32_t spl) = 0;
     virtual fcc_status variant_info(int32_t*, int32_t*, int32_t*, int32_t*, int32_t*, int32_t*) = 0;
     virtual fcc_status timing(double* ms, int64_t* launches, int64_t* body_steps) = 0;
+    virtual fcc_status tune(int64_t steps, bool reorder, int32_t* chosen, double* best_us) = 0;
+    virtual fcc_status graph_mode(int32_t enable, int32_t* active, int64_t* replays) = 0;
 };
 
 template <class T>
@@ -253,6 +255,14 @@ struct Pool final : PoolBase {
     long long* bld_h = nullptr;
     long long* stop_h = nullptr;
     GridSync* sy_h = nullptr;
+    int* fl_in_h = nullptr;  // release values uploaded at the start of a round
+    int* any_h = nullptr;
+    // CUDA graph of one round
+    bool use_graph = true, graph_ok = true;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    std::vector<long long> graph_key;
+    int64_t graph_launches = 0;
     // launch configuration
     int variant = -1;  // -1: default (variant 0)
     int spl = 512;
@@ -262,7 +272,9 @@ struct Pool final : PoolBase {
 
     ~Pool() override {
         if (stream) cudaStreamSynchronize(stream);
-        for (void* p : {(void*)fl_h, (void*)mc_h, (void*)clk_h, (void*)bld_h, (void*)stop_h, (void*)sy_h})
+        drop_graph();
+        for (void* p : {(void*)fl_h, (void*)mc_h, (void*)clk_h, (void*)bld_h, (void*)stop_h, (void*)sy_h,
+                        (void*)fl_in_h, (void*)any_h})
             if (p) cudaFreeHost(p);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -303,6 +315,8 @@ struct Pool final : PoolBase {
         CUDA_TRY(cudaMallocHost(&bld_h, nslots * sizeof(long long)));
         CUDA_TRY(cudaMallocHost(&stop_h, nslots * sizeof(long long)));
         CUDA_TRY(cudaMallocHost(&sy_h, sizeof(GridSync)));
+        CUDA_TRY(cudaMallocHost(&fl_in_h, nslots * sizeof(int)));
+        CUDA_TRY(cudaMallocHost(&any_h, sizeof(int)));
         A = std::make_unique<Arena<T>>();
         B = std::make_unique<Arena<T>>();
         const size_t nb = (size_t)max_bodies, nc = (size_t)max_cells;
@@ -574,14 +588,19 @@ struct Pool final : PoolBase {
         return FCC_OK;
     }
 
-    fcc_status read_status() {
+    // Status of every slot into pinned host buffers (queued on the stream).
+    fcc_status enqueue_status() {
         const int ns = nslots;
         CUDA_TRY(cudaMemcpyAsync(fl_h, flags.p, ns * sizeof(int), cudaMemcpyDeviceToHost, stream));
         CUDA_TRY(cudaMemcpyAsync(mc_h, maxcount.p, ns * sizeof(int), cudaMemcpyDeviceToHost, stream));
         CUDA_TRY(cudaMemcpyAsync(clk_h, clock.p, ns * sizeof(long long), cudaMemcpyDeviceToHost, stream));
         CUDA_TRY(cudaMemcpyAsync(bld_h, builds.p, ns * sizeof(long long), cudaMemcpyDeviceToHost, stream));
         CUDA_TRY(cudaMemcpyAsync(sy_h, sync.p, sizeof(GridSync), cudaMemcpyDeviceToHost, stream));
-        CUDA_TRY(cudaStreamSynchronize(stream));
+        return FCC_OK;
+    }
+
+    // Host mirror from the status read back (after the stream synchronised).
+    fcc_status process_status() {
         if (sy_h->error) return fail(FCC_ERR_DEVICE, "a grid barrier wait timed out in the step kernel");
         for (int s : order) {
             Slot& S = slots[s];
@@ -595,12 +614,17 @@ struct Pool final : PoolBase {
         return FCC_OK;
     }
 
-    // Release every simulation that has steps left up to min(n, horizon),
-    // with the rebuild decision bookkeeping() takes after a step
-    // (src/simulation.jl:132-142).  Returns the most steps any one needs.
-    fcc_status release(int64_t n, const std::vector<long long>& target, int64_t* most) {
+    // Release every simulation that has steps left up to its target, with
+    // the rebuild decision bookkeeping() takes after a step
+    // (src/simulation.jl:132-142), into the pinned upload buffers.  Returns the
+    // most steps any one needs.
+    int64_t release(const std::vector<long long>& target) {
         int any = 0;
-        *most = 0;
+        int64_t most = 0;
+        for (int s = 0; s < nslots; ++s) {
+            fl_in_h[s] = 0;
+            stop_h[s] = 0;
+        }
         for (int s : order) {
             Slot& S = slots[s];
             int f = S.flags_h & ~F_HOLD;
@@ -608,7 +632,7 @@ struct Pool final : PoolBase {
             if (target[s] <= S.clock_h) {
                 f |= F_HOLD;
             } else {
-                *most = std::max<int64_t>(*most, target[s] - S.clock_h);
+                most = std::max<int64_t>(most, target[s] - S.clock_h);
                 const bool need = (f & F_CONTACT) && !(f & F_FROZEN) &&
                                   ((f & F_REBUILD) || !(f & F_VALID) || (f & F_NEED) || S.spec.desc.skin == T(0));
                 if (need) {
@@ -617,23 +641,82 @@ struct Pool final : PoolBase {
                 }
             }
             S.flags_h = f;
-            fl_h[s] = f;
+            fl_in_h[s] = f;
         }
-        (void)n;
-        CUDA_TRY(cudaMemcpyAsync(flags.p, fl_h, nslots * sizeof(int), cudaMemcpyHostToDevice, stream));
-        CUDA_TRY(cudaMemcpyAsync(stop.p, stop_h, nslots * sizeof(long long), cudaMemcpyHostToDevice, stream));
-        CUDA_TRY(cudaMemcpyAsync(&sync.p->any_need, &any, sizeof(int), cudaMemcpyHostToDevice, stream));
-        return sync_stream();
+        *any_h = any;
+        return most;
     }
 
-    fcc_status launch(int nsteps) {
+    // One round: upload the release, `most` steps in launches of at most
+    // `spl` steps, download the status.  Recorded once as a CUDA graph and
+    // replayed while the launch configuration, the arena and the record
+    // parity are unchanged (the graph's copies read and write the pinned
+    // buffers, so new release values go in without re-recording).
+    fcc_status enqueue_round(int64_t most, long long g0) {
+        const int ns = nslots;
+        CUDA_TRY(cudaMemcpyAsync(flags.p, fl_in_h, ns * sizeof(int), cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(cudaMemcpyAsync(stop.p, stop_h, ns * sizeof(long long), cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(cudaMemcpyAsync(&sync.p->any_need, any_h, sizeof(int), cudaMemcpyHostToDevice, stream));
         DevPtrs<T> d = ptrs();
-        int p0 = par();
-        void* args[] = {&d, &nsteps, &p0};
-        CUDA_TRY(cudaLaunchCooperativeKernel(step_kernel(), dim3(grid), dim3(var().blk), args, stage_bytes(), stream));
-        gstep += nsteps;
-        ++last_launches;
-        return FCC_OK;
+        long long g = g0;
+        for (int64_t left = most; left > 0;) {
+            int k = (int)std::min<int64_t>(spl, left);
+            int p0 = (int)(g & 1);
+            void* args[] = {&d, &k, &p0};
+            CUDA_TRY(cudaLaunchCooperativeKernel(step_kernel(), dim3(grid), dim3(var().blk), args, stage_bytes(), stream));
+            g += k;
+            left -= k;
+        }
+        return enqueue_status();
+    }
+
+    fcc_status run_round(int64_t most) {
+        FCC_TRY(configure());
+        const int64_t nl = (most + spl - 1) / spl;
+        if (use_graph && graph_ok) {
+            const std::vector<long long> key = {(long long)(uintptr_t)A.get(), (long long)Ntot, (long long)Ctot,
+                                                (long long)grid, (long long)variant, (long long)split(),
+                                                (long long)cap, (long long)par(), (long long)most, (long long)spl};
+            if (key != graph_key) {
+                drop_graph();
+                cudaGraph_t g = nullptr;
+                CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+                const fcc_status st = enqueue_round(most, gstep);
+                const cudaError_t e = cudaStreamEndCapture(stream, &g);
+                if (st == FCC_OK && e == cudaSuccess && g &&
+                    cudaGraphInstantiate(&graph_exec, g, 0) == cudaSuccess) {
+                    graph = g;
+                    graph_key = key;
+                } else {
+                    // this runtime does not record the round (e.g. the
+                    // cooperative launch): launch it directly from now on
+                    if (g) cudaGraphDestroy(g);
+                    graph_exec = nullptr;
+                    graph_ok = false;
+                    cudaGetLastError();
+                }
+            }
+            if (graph_ok) {
+                CUDA_TRY(cudaGraphLaunch(graph_exec, stream));
+                ++graph_launches;
+            } else {
+                FCC_TRY(enqueue_round(most, gstep));
+            }
+        } else {
+            FCC_TRY(enqueue_round(most, gstep));
+        }
+        gstep += most;
+        last_launches += nl;
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        return process_status();
+    }
+
+    void drop_graph() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (graph) cudaGraphDestroy(graph);
+        graph_exec = nullptr;
+        graph = nullptr;
+        graph_key.clear();
     }
 
     // Neighbour-list overflow of some simulations: regrow the shared capacity
@@ -653,31 +736,16 @@ struct Pool final : PoolBase {
         return FCC_OK;
     }
 
-    fcc_status run(int64_t n) override {
-        last_launches = 0;
-        last_body_steps = 0;
-        last_ms = 0;
-        if (n <= 0) return FCC_OK;
-        FCC_TRY(compact());
-        std::vector<long long> target(nslots, 0);
-        for (int s : order) {
-            const Slot& S = slots[s];
-            target[s] = S.clock_h + std::min<long long>(n, std::max<long long>(0, S.horizon - S.clock_h));
-        }
-        CUDA_TRY(cudaEventRecord(ev0, stream));
+    // Advance every simulation to its target clock (rounds until no
+    // simulation is frozen by a list overflow); all hold afterwards.
+    fcc_status advance_to(const std::vector<long long>& target) {
         for (int round = 0;; ++round) {
-            int64_t most = 0;
-            FCC_TRY(release(n, target, &most));
+            const int64_t most = release(target);
             if (most == 0) break;
-            FCC_TRY(configure());
-            for (int64_t left = most; left > 0;) {
-                const int k = (int)std::min<int64_t>(spl, left);
-                FCC_TRY(launch(k));
-                left -= k;
-            }
-            FCC_TRY(read_status());
+            FCC_TRY(run_round(most));
             bool frozen = false;
             for (int s : order) frozen |= (slots[s].flags_h & F_FROZEN) != 0;
+            if (frozen && tuning) return fail(FCC_ERR_FULL, "pool: a neighbour list overflowed during tuning");
             if (frozen) FCC_TRY(regrow());
             else {
                 for (int s : order)
@@ -687,15 +755,185 @@ struct Pool final : PoolBase {
             }
             if (round > 64) return fail(FCC_ERR_DEVICE, "pool: neighbour lists did not fit after regrowth");
         }
-        // everything holds until the next run
         for (int s : order) slots[s].flags_h |= F_HOLD;
-        for (int s : order) fl_h[s] = slots[s].flags_h;
-        CUDA_TRY(cudaMemcpyAsync(flags.p, fl_h, nslots * sizeof(int), cudaMemcpyHostToDevice, stream));
+        for (int s = 0; s < nslots; ++s) fl_in_h[s] = 0;
+        for (int s : order) fl_in_h[s] = slots[s].flags_h;
+        CUDA_TRY(cudaMemcpyAsync(flags.p, fl_in_h, nslots * sizeof(int), cudaMemcpyHostToDevice, stream));
+        return sync_stream();
+    }
+
+    fcc_status run(int64_t n) override {
+        last_launches = 0;
+        last_body_steps = 0;
+        last_ms = 0;
+        if (n <= 0) return FCC_OK;
+        FCC_TRY(compact());
+        FCC_TRY(apply_tuned());
+        std::vector<long long> target(nslots, 0);
+        for (int s : order) {
+            const Slot& S = slots[s];
+            target[s] = S.clock_h + std::min<long long>(n, std::max<long long>(0, S.horizon - S.clock_h));
+        }
+        CUDA_TRY(cudaEventRecord(ev0, stream));
+        FCC_TRY(advance_to(target));
         CUDA_TRY(cudaEventRecord(ev1, stream));
         CUDA_TRY(cudaEventSynchronize(ev1));
         float ms = 0;
         CUDA_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
         last_ms = ms;
+        return FCC_OK;
+    }
+
+    // ------------------------------------------------------- autotuner --
+    // Launch shapes are chosen per size bucket (packed bodies rounded up to a
+    // power of two, precision): each candidate variant runs `steps` steps of
+    // the live pool from a snapshot, the fastest is kept, and the snapshot is
+    // restored, so tuning leaves no trace in the trajectories.  By default the
+    // candidates are the variants with the current lanes x node slots (block
+    // size and register budget differ; the arithmetic and its order do not,
+    // so results stay bit-identical); `reorder` admits every variant (other
+    // lane counts sum node quadratures in another order: results then agree
+    // with the default to FP32 rounding, not bit for bit).
+    static std::map<std::pair<int, int>, int>& tune_table() {
+        static std::map<std::pair<int, int>, int> t;
+        return t;
+    }
+    static std::mutex& tune_mutex() {
+        static std::mutex m;
+        return m;
+    }
+    std::pair<int, int> bucket() const {
+        int b = 0;
+        while ((1ll << b) < std::max<int64_t>(Ntot, 1)) ++b;
+        return {(int)sizeof(T), b};
+    }
+    bool tuned = false;     // variant came from the table or a tune call
+    bool tuning = false;    // inside a tune trial (the snapshot in B must survive)
+    bool user_set = false;  // fcc_pool_config chose the variant
+
+    fcc_status apply_tuned() {
+        if (user_set) return FCC_OK;
+        std::lock_guard<std::mutex> lk(tune_mutex());
+        auto it = tune_table().find(bucket());
+        if (it != tune_table().end()) {
+            variant = it->second;
+            tuned = true;
+        } else {
+            variant = -1;
+            tuned = false;
+        }
+        return FCC_OK;
+    }
+
+    // Identity copy of the live arena ranges from one copy to the other.
+    fcc_status copy_arena(Arena<T>& src, Arena<T>& dst) {
+        if (dst.cap != src.cap || dst.ccap != src.ccap || dst.bcap != src.bcap)
+            FCC_TRY(dst.alloc((size_t)max_bodies, (size_t)max_cells, src.cap, src.ccap, src.bcap, stream));
+        std::vector<MoveRange> mv;
+        for (int s : order) {
+            const Slot& S = slots[s];
+            mv.push_back(MoveRange{(int)S.off, (int)S.off, (int)S.npad, S.coff, S.coff, S.ncells});
+        }
+        if (mv.empty()) return FCC_OK;
+        CUDA_TRY(cudaMemcpyAsync(moves.p, mv.data(), mv.size() * sizeof(MoveRange), cudaMemcpyHostToDevice, stream));
+        if (Ntot > 0)
+            k_pool_gather_bodies<T><<<(int)((Ntot + 255) / 256), 256, 0, stream>>>(src.ptrs(), dst.ptrs(), moves.p,
+                                                                                 (int)mv.size(), (int)Ntot, par());
+        if (Ctot > 0)
+            k_pool_gather_cells<T><<<(int)((Ctot + 255) / 256), 256, 0, stream>>>(src.ptrs(), dst.ptrs(), moves.p,
+                                                                                (int)mv.size(), (int)Ctot);
+        CUDA_TRY(cudaGetLastError());
+        return sync_stream();
+    }
+
+    fcc_status graph_mode(int32_t enable, int32_t* active, int64_t* replays) override {
+        if (enable >= 0) {
+            use_graph = enable != 0;
+            drop_graph();
+        }
+        if (active) *active = (use_graph && graph_ok) ? 1 : 0;
+        if (replays) *replays = graph_launches;
+        return FCC_OK;
+    }
+
+    fcc_status tune(int64_t steps, bool reorder, int32_t* chosen, double* best_us) override {
+        FCC_TRY(compact());
+        if (order.empty()) return fail(FCC_ERR_ARGUMENT, "pool: nothing to tune on (no simulations)");
+        if (steps < 1) return fail(FCC_ERR_ARGUMENT, "pool: tune needs at least one step");
+        // snapshot: arena into B, per-slot device state and the host mirror
+        FCC_TRY(copy_arena(*A, *B));
+        const int ns = nslots;
+        std::vector<int> f0(ns), m0(ns);
+        std::vector<long long> c0(ns), b0(ns), st0(ns);
+        CUDA_TRY(cudaMemcpyAsync(f0.data(), flags.p, ns * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaMemcpyAsync(m0.data(), maxcount.p, ns * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaMemcpyAsync(c0.data(), clock.p, ns * sizeof(long long), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaMemcpyAsync(b0.data(), builds.p, ns * sizeof(long long), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaMemcpyAsync(st0.data(), stop.p, ns * sizeof(long long), cudaMemcpyDeviceToHost, stream));
+        FCC_TRY(sync_stream());
+        const std::vector<Slot> mirror = slots;
+        const long long gstep0 = gstep;
+        const int cap0 = cap, variant0 = variant;
+        const Variant& cur = VARIANTS[variant < 0 ? 0 : variant];
+        auto restore = [&]() -> fcc_status {
+            if (A->cap != cap0) {
+                FCC_TRY(A->alloc((size_t)max_bodies, (size_t)max_cells, cap0, ccap, bcap, stream));
+            }
+            cap = cap0;
+            gstep = gstep0;
+            FCC_TRY(copy_arena(*B, *A));
+            slots = mirror;
+            CUDA_TRY(cudaMemcpyAsync(flags.p, f0.data(), ns * sizeof(int), cudaMemcpyHostToDevice, stream));
+            CUDA_TRY(cudaMemcpyAsync(maxcount.p, m0.data(), ns * sizeof(int), cudaMemcpyHostToDevice, stream));
+            CUDA_TRY(cudaMemcpyAsync(clock.p, c0.data(), ns * sizeof(long long), cudaMemcpyHostToDevice, stream));
+            CUDA_TRY(cudaMemcpyAsync(builds.p, b0.data(), ns * sizeof(long long), cudaMemcpyHostToDevice, stream));
+            CUDA_TRY(cudaMemcpyAsync(stop.p, st0.data(), ns * sizeof(long long), cudaMemcpyHostToDevice, stream));
+            for (int s = 0; s < nslots; ++s) fl_in_h[s] = f0[s];
+            return sync_stream();
+        };
+        int best = -1;
+        double best_t = 1e300;
+        for (int v = 0; v < NVARIANTS; ++v) {
+            const Variant& c = VARIANTS[v];
+            if (sizeof(T) != 4 && !c.f64) continue;
+            if (!reorder && (c.L != cur.L || c.S != cur.S)) continue;
+            variant = v;
+            drop_graph();
+            std::vector<long long> target(nslots, 0);
+            for (int s : order) target[s] = slots[s].clock_h + steps;
+            CUDA_TRY(cudaEventRecord(ev0, stream));
+            tuning = true;
+            const fcc_status st = advance_to(target);
+            tuning = false;
+            CUDA_TRY(cudaEventRecord(ev1, stream));
+            CUDA_TRY(cudaEventSynchronize(ev1));
+            float ms = 0;
+            CUDA_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
+            FCC_TRY(restore());
+            if (st == FCC_ERR_FULL) {  // lists must regrow first: leave the launch shape untuned
+                drop_graph();
+                variant = variant0;
+                if (chosen) *chosen = -1;
+                if (best_us) *best_us = 0;
+                return FCC_OK;
+            }
+            if (st != FCC_OK) return st;
+            if (ms < best_t) {
+                best_t = ms;
+                best = v;
+            }
+        }
+        drop_graph();
+        variant = variant0;
+        if (best < 0) return fail(FCC_ERR_UNSUPPORTED, "pool: no kernel variant to tune");
+        {
+            std::lock_guard<std::mutex> lk(tune_mutex());
+            tune_table()[bucket()] = best;
+        }
+        user_set = false;
+        FCC_TRY(apply_tuned());
+        if (chosen) *chosen = best;
+        if (best_us) *best_us = best_t * 1e3 / (double)steps;
         return FCC_OK;
     }
 
@@ -808,7 +1046,9 @@ struct Pool final : PoolBase {
             return fail(FCC_ERR_UNSUPPORTED, "pool: this kernel variant has no FP64 build");
         if (steps < 0) return fail(FCC_ERR_ARGUMENT, "pool: steps per launch must be >= 0");
         variant = v;
+        user_set = v >= 0;
         spl = steps > 0 ? steps : 512;
+        drop_graph();
         return FCC_OK;
     }
 
@@ -915,6 +1155,12 @@ fcc_status fcc_pool_variant(fcc_pool* pool, int32_t* variant, int32_t* lanes, in
 }
 fcc_status fcc_pool_last_timing(fcc_pool* pool, double* ms, int64_t* launches, int64_t* body_steps) {
     POOL_CALL(timing(ms, launches, body_steps));
+}
+fcc_status fcc_pool_tune(fcc_pool* pool, int64_t steps, int32_t reorder, int32_t* variant, double* us_per_step) {
+    POOL_CALL(tune(steps, reorder != 0, variant, us_per_step));
+}
+fcc_status fcc_pool_graph(fcc_pool* pool, int32_t enable, int32_t* active, int64_t* replays) {
+    POOL_CALL(graph_mode(enable, active, replays));
 }
 
 }  // extern "C"

@@ -39,6 +39,8 @@ _POOL_SIG = {
     "pool_config": [C.c_void_p, C.c_int32, C.c_int32],
     "pool_variant": [C.c_void_p] + [C.POINTER(C.c_int32)] * 6,
     "pool_last_timing": [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
+    "pool_tune": [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)],
+    "pool_graph": [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int64)],
 }
 
 
@@ -223,6 +225,21 @@ class Pool:
         v = [C.c_int32() for _ in range(6)]
         self._call("pool_variant", self._h, *(C.byref(x) for x in v))
         return dict(zip(("variant", "lanes", "slots", "block", "min_blocks", "grid"), (x.value for x in v)))
+
+    def tune(self, steps: int = 64, reorder: bool = False):
+        """Autotune the launch shape for this pool's size bucket (from a
+        snapshot, restored afterwards); returns (variant, µs per step) or
+        (-1, 0) when nothing could be tuned yet."""
+        v, us = C.c_int32(), C.c_double()
+        self._call("pool_tune", self._h, int(steps), 1 if reorder else 0, C.byref(v), C.byref(us))
+        return v.value, us.value
+
+    def graph(self, enable=None):
+        """CUDA-graph replay of run rounds: switch on/off (None: query).
+        Returns (active, replays)."""
+        a, r = C.c_int32(), C.c_int64()
+        self._call("pool_graph", self._h, -1 if enable is None else int(bool(enable)), C.byref(a), C.byref(r))
+        return bool(a.value), r.value
 
     def last_timing(self):
         """(device ms, kernel launches, body-steps) of the last run."""

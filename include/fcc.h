@@ -316,6 +316,24 @@ fcc_status fcc_pool_variant(fcc_pool* pool, int32_t* variant, int32_t* lanes, in
  * body-steps executed (summed over simulations). */
 fcc_status fcc_pool_last_timing(fcc_pool* pool, double* ms, int64_t* launches, int64_t* body_steps);
 
+/* Autotuner: time every candidate kernel variant for `steps` steps of the
+ * pool's current simulations, from a snapshot that is restored afterwards
+ * (tuning leaves the trajectories untouched), and keep the fastest for this
+ * size bucket (packed bodies rounded up to a power of two) in a process-wide
+ * table that later runs of any pool of that bucket use unless fcc_pool_config
+ * fixed a variant.  reorder = 0: only variants with the current lanes x node
+ * slots (results stay bit-identical); 1: every variant (node quadratures then
+ * sum in another order: results agree to FP32 rounding).  *variant = -1 when
+ * a neighbour list would have to regrow first (nothing tuned). */
+fcc_status fcc_pool_tune(fcc_pool* pool, int64_t steps, int32_t reorder, int32_t* variant, double* us_per_step);
+
+/* CUDA graph of a run round (release upload, persistent launches, status
+ * download), recorded once per launch configuration and replayed:
+ * enable = 1 / 0 switches it on (default) / off, -1 only queries.  *active = 0
+ * when off or when this runtime could not record the round (then rounds are
+ * launched directly); *replays counts graph launches. */
+fcc_status fcc_pool_graph(fcc_pool* pool, int32_t enable, int32_t* active, int64_t* replays);
+
 /* Message of the last error on this thread. */
 const char* fcc_last_error(void);
 

@@ -160,3 +160,47 @@ def test_pool_typed_bodies_with_parent_drag():
     pool.run(80)
     for s, (b, box, kw) in zip(slots, out):
         assert_same(pool, s, alone(b, box, kw, T, 80))
+
+
+def test_pool_graph_replay_equals_direct_launches():
+    """Rounds replayed from a recorded CUDA graph equal direct launches."""
+    T = np.float32
+    ms = members(T, fast=True)
+    pools = [fcc.Pool(T=T, max_bodies=4096, max_cells=4096, max_sims=8) for _ in range(2)]
+    pools[1].graph(False)
+    slots = [[p.add(b, box, horizon=10**6, **kw) for b, box, kw in ms] for p in pools]
+    for p in pools:
+        for _ in range(4):
+            p.run(64)  # equal rounds: recorded once, then replayed
+    active, replays = pools[0].graph()
+    assert pools[1].graph() == (False, 0)
+    if active:
+        assert replays >= 4
+    for s0, s1 in zip(*slots):
+        a, b = pools[0].bodies(s0), pools[1].bodies(s1)
+        for f in ("x", "y", "θ", "coef", "imgx", "imgy"):
+            assert np.array_equal(getattr(a, f), getattr(b, f)), f
+
+
+def test_pool_tune_leaves_no_trace():
+    """The autotuner times variants from a snapshot and restores it: a tuned
+    pool continues exactly like an untuned one (result-invariant candidates)."""
+    T = np.float32
+    ms = members(T, fast=True)
+    pa = fcc.Pool(T=T, max_bodies=4096, max_cells=4096, max_sims=8)
+    pb = fcc.Pool(T=T, max_bodies=4096, max_cells=4096, max_sims=8)
+    sa = [pa.add(b, box, horizon=400, **kw) for b, box, kw in ms]
+    sb = [pb.add(b, box, horizon=400, **kw) for b, box, kw in ms]
+    pa.run(100)
+    pb.run(100)
+    v, us = pa.tune(32)
+    assert v in (0, 3) and us > 0          # variants sharing 8 lanes x 5 node slots
+    assert pa.variant()["lanes"] == 8
+    pa.run(300)
+    pb.run(300)
+    for x, y in zip(sa, sb):
+        a, b = pa.state(x), pb.state(y)
+        assert a[1:] == b[1:]
+        for f in ("x", "y", "θ", "coef", "imgx", "imgy"):
+            assert np.array_equal(getattr(a[0], f), getattr(b[0], f)), f
+        assert pa.builds(x) == pb.builds(y)
