@@ -118,7 +118,8 @@ struct DevPtrs {
     long long* builds;
     int* maxcount;
     GridSync* sync;
-    const T* cs;  // cos/sin of the node angles, 2*nth
+    const T* cs;     // cos/sin of the node angles, 2*nth
+    const T* basis;  // [nth][KM][4]: cos n phi_k, sin n phi_k, n cos n phi_k, n sin n phi_k (n = 2..10)
     // forces of the split (parent drag) step and of compute_gradients
     T* gx;
     T* gy;
@@ -158,9 +159,12 @@ __device__ __forceinline__ void t_sincos(double a, double* s, double* c) { sinco
 __device__ __forceinline__ float t_pi(float*) { return 3.14159265358979323846f; }
 __device__ __forceinline__ double t_pi(double*) { return 3.14159265358979323846; }
 
-// minimum_image, src/box.jl:14, exactly rounded as the reference evaluates it
+// minimum_image, src/box.jl:14, exactly rounded as the reference evaluates it.
+// For |d| < L/2 the rounded quotient is at most 1/2 and rint gives ±0, so the
+// result is d - (±0) = d + 0: returned without the division (same bits).
 template <class T>
 __device__ __forceinline__ T minimum_image_exact(T d, T L) {
+    if (fabs(d) < T(0.5) * L) return add_rn(d, T(0));
     return sub_rn(d, mul_rn(L, t_rint(div_rn(d, L))));
 }
 // minimum image with a precomputed 1/L (force evaluation; differs from the
@@ -171,9 +175,16 @@ __device__ __forceinline__ T minimum_image_fast(T d, T L, T invL) {
     return d - L * t_rint(d * invL);
 }
 
-// wrap, src/box.jl:21-30
+// wrap, src/box.jl:21-30.  For 0 <= x < L the rounded quotient x/L stays
+// below 1 (the largest value below L is at least one ulp of 1 away), so the
+// floor is 0 and the result is x - 0 = x + 0: returned without the division
+// (same bits).
 template <class T>
 __device__ __forceinline__ T wrap_exact(T x, T L, int& shift) {
+    if (x >= T(0) && x < L) {
+        shift = 0;
+        return add_rn(x, T(0));
+    }
     T s = t_floor(div_rn(x, L));
     T xp = sub_rn(x, mul_rn(s, L));
     if (xp >= L) {
@@ -267,6 +278,9 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// wait until at most N of this thread's committed copy groups are pending
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // ------------------------------------------------------------ grid barrier
 // Barrier over all blocks of a cooperative launch (all co-resident).  Arrival
@@ -297,6 +311,12 @@ __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+#ifndef FCC_BARRIER_FENCE
+#define FCC_BARRIER_FENCE 0  // 1: full fence before the release store (measured: not needed, 1% slower)
+#endif
+#ifndef FCC_BARRIER_SLEEP
+#define FCC_BARRIER_SLEEP 20  // ns between polls of the generation word
+#endif
 template <class F>
 __device__ __forceinline__ bool grid_barrier(GridSync* gs, F&& last) {
     __shared__ int s_last, s_err;
@@ -314,8 +334,10 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, F&& last) {
         __syncthreads();
         if (threadIdx.x == 0) {
             gs->count = 0;
+#if FCC_BARRIER_FENCE
             __threadfence();
-            st_release(&gs->gen, gen + 1);
+#endif
+            st_release(&gs->gen, gen + 1);  // release: the reset and the block's writes before it
         }
     } else if (threadIdx.x == 0) {
         long long it = 0;
@@ -325,7 +347,9 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, F&& last) {
                 s_err = 1;
                 break;
             }
-            __nanosleep(20);
+#if FCC_BARRIER_SLEEP > 0
+            __nanosleep(FCC_BARRIER_SLEEP);
+#endif
         }
     }
     __syncthreads();

@@ -96,6 +96,10 @@ __device__ __forceinline__ float4 lds4(const float* p) {
     asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
     return v;
 }
+struct Double4 {
+    double x, y, z, w;
+};
+__device__ __forceinline__ Double4 lds4(const double* p) { return Double4{p[0], p[1], p[2], p[3]}; }
 __device__ __forceinline__ void lds_head(const float* p, float& x, float& y, float& rm, float& w) {
     const float4 v = lds4(p);
     x = v.x, y = v.y, rm = v.z, w = v.w;
@@ -349,9 +353,27 @@ __device__ void phase_neighbors(const DevPtrs<T>& d, int par, int tid, int nthr)
 // L2 in the loop).  At packing 0.95 with the 0.3 skin a body lists 6-9.
 constexpr int NBMAX = 12;
 
+// FP32 single-chunk kernels read cos(n phi_k), sin(n phi_k) (and n times
+// them) of their contour nodes from a shared-memory table instead of running
+// the angle-addition recurrence: four floats per node and mode, a node's row
+// 36 words apart (conflict-free float4 reads for the 8 nodes a warp reads).
+constexpr int BASIS_NODES = 40;
+#ifndef FCC_HIT_PAIRS
+#define FCC_HIT_PAIRS 0  // 1: the contact walk evaluates two hits per iteration
+#endif
+#ifndef FCC_MODE_TABLE
+#define FCC_MODE_TABLE 2  // 1: synthesis reads the table, 2: pullback (measured fastest), 3: both
+#endif
+template <class T>
+__host__ __device__ constexpr size_t basis_table_bytes() {
+    return sizeof(T) == 4 ? (size_t)BASIS_NODES * KM * 4 * sizeof(T) : 0;
+}
+
+// Per warp: the own records of its 32/L bodies, then NBMAX neighbour
+// records per body.
 template <class T, int L>
 __host__ __device__ constexpr size_t stage_bytes_per_warp() {
-    return (size_t)(32 / L) * NBMAX * RECW * sizeof(T);
+    return (size_t)(32 / L) * (1 + NBMAX) * RECW * sizeof(T);
 }
 
 // Operands of the update loaded early (their latency overlaps the force
@@ -435,13 +457,12 @@ __device__ __forceinline__ void substrate_displacement(const DevPtrs<T>& d, cons
 // are the group-reduced gradients (uniform across the group).
 template <class T, int L>
 __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T>& P, bool act, int g, int s, int l,
-                                            int par, long long clk, const T (&rv)[RECW], T r0, int ti, T fx, T fy,
+                                            int par, long long clk, T xo, T yo, T wo, T tho, T r0, int ti, T fx, T fy,
                                             T tt, const T (&gl)[NCM], const UpdatePre<T, L>& pre, int fl,
                                             const T (&nz)[2], bool split) {
     constexpr unsigned FULL = 0xffffffffu;
     constexpr int MPL = UpdatePre<T, L>::MPL;
     const T dt = P.dt;
-    const T tho = rv[R_TH];
     const uint32_t li = (uint32_t)(g - P.body_off + 1);
     // standard normals of this body and step (src/random.jl:88-100): lane 0
     // holds block 1 (orientation), lane 1 block 0 (translation)
@@ -527,7 +548,7 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
         if (split) {
             const T* rc = rec_cur(d, par);
             if (P.parent_drag[ti]) {
-                const int c = unpack_w(rv[R_W]) >> 3;
+                const int c = unpack_w(wo) >> 3;
                 T ux, uy;
                 substrate_displacement(d, P, rc, c, clk, ux, uy);
                 const T sig = t_sqrt(T(2) * P.Dt[ti] * dt);
@@ -542,14 +563,14 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
             dyp = dt * (P.v0[ti] * so1 - P.mur[ti] * fy) + sig * xi2;
         }
         int sx, sy;
-        const T xw = wrap_exact(add_rn(rv[R_X], dxp), P.Lx, sx);
-        const T yw = wrap_exact(add_rn(rv[R_Y], dyp), P.Ly, sy);
-        d.imgx[g] += sx;
-        d.imgy[g] += sy;
+        const T xw = wrap_exact(add_rn(xo, dxp), P.Lx, sx);
+        const T yw = wrap_exact(add_rn(yo, dyp), P.Ly, sy);
+        if (sx) d.imgx[g] += sx;  // image counters change only on a wrap
+        if (sy) d.imgy[g] += sy;
         rn[R_X] = xw;
         rn[R_Y] = yw;
         rn[R_RMAX] = rmax;
-        rn[R_W] = rv[R_W];
+        rn[R_W] = wo;
         rn[R_A0] = r0 * a0n;
         rn[R_TH] = thn;
         cf[0] = a0n;
@@ -575,6 +596,12 @@ __device__ __forceinline__ void carry_record(const DevPtrs<T>& d, int g, int l, 
     for (int u = 0; u < RECW; ++u)
         if ((u & (L - 1)) == l) rn[u] = rv[u];
 }
+// the same from the record staged in shared memory
+template <class T, int L>
+__device__ __forceinline__ void carry_record_staged(const DevPtrs<T>& d, int g, int l, int par, const T* own) {
+    T* rn = rec_next(d, par) + (size_t)g * RECW;
+    for (int u = l; u < RECW; u += L) rn[u] = own[u];
+}
 
 // ==================================================== force evaluation ==
 enum : int { MODE_FUSED = 0, MODE_FORCES = 1, MODE_DIAG = 2 };
@@ -589,11 +616,16 @@ enum : int { MODE_FUSED = 0, MODE_FORCES = 1, MODE_DIAG = 2 };
 //   bond forces                                 src/energies/bonds.jl:98-111
 //   pullback glab = S' Gall                     src/gradients.jl:374-386
 template <class T, int L, int S, bool ONE, int MODE>
-__device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stage, int par, const SimDesc<T>* sim0) {
+__device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stage, int par, const SimDesc<T>* sim0,
+                                            const T* tab) {
     constexpr int BPW = 32 / L;
     constexpr unsigned FULL = 0xffffffffu;
     constexpr int CH16 = RECW * (int)sizeof(T) / 16;  // 16-byte chunks per record
     constexpr int IDS = (NBMAX + L - 1) / L;           // staged neighbour ids per lane
+    // the mode table is staged (stage_basis); synthesis and pullback may use it
+    constexpr bool USE_TAB = ONE && sizeof(T) == 4;
+    constexpr bool TAB_SYNTH = USE_TAB && (FCC_MODE_TABLE & 1);
+    constexpr bool TAB_PULL = USE_TAB && (FCC_MODE_TABLE & 2);
     const int lane = threadIdx.x & 31;
     const int l = lane & (L - 1);
     const int g = wg * BPW + lane / L;
@@ -610,10 +642,17 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
     const bool valid = sim0 ? g < d.Ntot : g < P.body_off + P.n;
     const int gg = valid ? g : (sim0 ? 0 : wg * BPW);
     const T* rc = rec_cur(d, par);
-    // ---- independent loads first: own record, neighbour count and ids,
+    // ---- independent loads first: own record (centre, tag, a0 and theta to
+    // registers, the whole record to shared memory), neighbour count and ids,
     // simulation state, update operands
-    T rv[RECW];
-    load_rec(rc + (size_t)gg * RECW, rv);
+    T* own = stage + (size_t)(lane / L) * RECW;
+    T* snb = stage + (size_t)BPW * RECW + (size_t)(lane / L) * NBMAX * RECW;
+    const T* grec = rc + (size_t)gg * RECW;
+    T xi, yi, rmi, wf;
+    load_head(grec, xi, yi, rmi, wf);
+    const T a0r = ldcg(grec + R_A0), th = ldcg(grec + R_TH);
+    for (int c = l; c < CH16; c += L) cp_async16(own + c * (16 / sizeof(T)), grec + c * (16 / sizeof(T)));
+    cp_async_commit();
     const T r0 = __ldg(d.R0 + gg);
     const int cnt_raw = ldcg(d.nb_count + gg);
     int ids[IDS];
@@ -641,7 +680,6 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
     // ---- stage the neighbour records in shared memory (cp.async)
     const bool contact = act && (fl & F_CONTACT);
     const int cnt = contact ? min(cnt_raw, d.cap) : 0;
-    T* snb = stage + (size_t)(lane / L) * NBMAX * RECW;
     auto stage_batch = [&](int base) {
         const int npre = min(cnt - base, NBMAX);
         __syncwarp();  // every lane is done with the previous contents
@@ -660,7 +698,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
     stage_batch(0);
     int staged_base = 0;
 
-    const int wv = unpack_w(rv[R_W]);
+    const int wv = unpack_w(wf);
     const int ti = wv & 7;
     const int pi = wv >> 3;
 
@@ -668,8 +706,11 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
     unsigned vmask = 0;
     const int nch = ONE ? 1 : (nth + L * S - 1) / (L * S);
 
+    // own lab coefficients are read from the staged record (modes outer,
+    // nodes inner; per node the same operations as one recurrence per node)
     auto synth = [&](int ch) {
         vmask = 0;
+        T cc[S], ss[S];
 #pragma unroll
         for (int sl = 0; sl < S; ++sl) {
             const int k = ch * L * S + l + L * sl;
@@ -678,23 +719,39 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
             const T s1 = v ? __ldg(d.cs + 2 * k + 1) : T(0);
             C1[sl] = c1;
             S1[sl] = s1;
-            T c = c1, sn = s1, r = rv[R_A0], r1 = T(0);
-#pragma unroll
-            for (int m = 0; m < KM; ++m) {
-                const T n = T(m + 2);
-                const T cn = c * c1 - sn * s1;
-                sn = sn * c1 + c * s1;
-                c = cn;
-                const T al = rv[r_al(m)], be = rv[r_be(m)];
-                r += al * c + be * sn;
-                r1 += n * (be * c - al * sn);
-            }
-            R[sl] = v ? r : T(0);
-            R1[sl] = v ? r1 : T(0);
+            cc[sl] = c1;
+            ss[sl] = s1;
+            R[sl] = a0r;
+            R1[sl] = T(0);
             if (v) vmask |= 1u << sl;
         }
+#pragma unroll
+        for (int m = 0; m < KM; ++m) {
+            const T al = own[r_al(m)], be = own[r_be(m)];
+            const T n = T(m + 2);
+#pragma unroll
+            for (int sl = 0; sl < S; ++sl) {
+                if constexpr (TAB_SYNTH) {
+                    const int k = l + L * sl;
+                    const auto t = lds4(tab + ((vmask & (1u << sl)) ? k : 0) * KM * 4 + m * 4);
+                    R[sl] += al * t.x + be * t.y;
+                    R1[sl] += be * t.z - al * t.w;
+                } else {
+                    const T cn = cc[sl] * C1[sl] - ss[sl] * S1[sl];
+                    ss[sl] = ss[sl] * C1[sl] + cc[sl] * S1[sl];
+                    cc[sl] = cn;
+                    R[sl] += al * cc[sl] + be * ss[sl];
+                    R1[sl] += n * (be * cc[sl] - al * ss[sl]);
+                }
+            }
+        }
+#pragma unroll
+        for (int sl = 0; sl < S; ++sl)
+            if (!(vmask & (1u << sl))) R[sl] = R1[sl] = T(0);
     };
 
+    cp_async_wait_group<1>();  // the own record (the neighbour copies may still fly)
+    __syncwarp();
     // ---- pass 1: contour integral Q = sum_k sqrt(R^2 + R'^2) dphi
     T Qp = T(0);
     for (int ch = 0; ch < nch; ++ch) {
@@ -738,7 +795,6 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
     cp_async_wait_all();
     __syncwarp();
     const int maxc = __reduce_max_sync(FULL, cnt);
-    const T xi = rv[R_X], yi = rv[R_Y];
     const T Lx = P.Lx, Ly = P.Ly, iLx = P.invLx, iLy = P.invLy, crange = P.crange;
     const bool rewrap = P.rewrap != 0;
 
@@ -786,11 +842,10 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                     // (2) every lane walks its own hits in (neighbour, node) order, so
                     // each node sums its neighbours' g(d) in list order
                     // (src/energies/contact.jl:309-322)
-                    while (hm) {
-                        const int bit = __ffsll((long long)hm) - 1;
-                        hm &= hm - 1;
+                    // g(d) of one hit (bit (q - q0) * S + slot of the mask)
+                    auto hit_value = [&](int bit, int& sl) -> T {
                         const int qq = q0 + bit / S;
-                        const int sl = bit - (bit / S) * S;
+                        sl = bit - (bit / S) * S;
                         const T* nrec = snb + qq * RECW;
                         T xj, yj, rmj, wj;
                         lds_head(nrec, xj, yj, rmj, wj);
@@ -817,10 +872,39 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                         const int wjv = unpack_w(wj);
                         T gv = dd >= T(0) ? P.cA[(wjv >> 3) == pi ? 1 : 0][ti][wjv & 7] : T(0);
                         if (dd > T(0)) gv += P.cB[ti] * dd;
+                        return gv;
+                    };
+#if FCC_HIT_PAIRS
+                    // two hits per iteration (independent chains), added in bit order
+                    while (hm) {
+                        const int ba = __ffsll((long long)hm) - 1;
+                        hm &= hm - 1;
+                        const bool two = hm != 0;
+                        const int bb = two ? __ffsll((long long)hm) - 1 : ba;
+                        if (two) hm &= hm - 1;
+                        int sa, sb;
+                        const T ga = hit_value(ba, sa);
+                        const T gb = hit_value(bb, sb);
+#pragma unroll
+                        for (int u = 0; u < S; ++u)
+                            if (sa == u) p[u] += ga;
+                        if (two) {
+#pragma unroll
+                            for (int u = 0; u < S; ++u)
+                                if (sb == u) p[u] += gb;
+                        }
+                    }
+#else
+                    while (hm) {
+                        const int bit = __ffsll((long long)hm) - 1;
+                        hm &= hm - 1;
+                        int sl;
+                        const T gv = hit_value(bit, sl);
 #pragma unroll
                         for (int u = 0; u < S; ++u)
                             if (sl == u) p[u] += gv;
                     }
+#endif
                 }
             }
         }
@@ -842,15 +926,25 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
             fy += pw * (r * s1 - r1 * c1);
             tt += (-pw * r) * r1;
             gl[0] += GRk;
-            T c = c1, sn = s1;
+            if constexpr (TAB_PULL) {
+                const int k = l + L * sl;
 #pragma unroll
-            for (int m = 0; m < KM; ++m) {
-                const T n = T(m + 2);
-                const T cn = c * c1 - sn * s1;
-                sn = sn * c1 + c * s1;
-                c = cn;
-                gl[1 + m] += c * GRk - n * sn * GDk;
-                gl[1 + KM + m] += sn * GRk + n * c * GDk;
+                for (int m = 0; m < KM; ++m) {
+                    const auto t = lds4(tab + (k * KM + m) * 4);
+                    gl[1 + m] += t.x * GRk - t.w * GDk;
+                    gl[1 + KM + m] += t.y * GRk + t.z * GDk;
+                }
+            } else {
+                T c = c1, sn = s1;
+#pragma unroll
+                for (int m = 0; m < KM; ++m) {
+                    const T n = T(m + 2);
+                    const T cn = c * c1 - sn * s1;
+                    sn = sn * c1 + c * s1;
+                    c = cn;
+                    gl[1 + m] += c * GRk - n * sn * GDk;
+                    gl[1 + KM + m] += sn * GRk + n * c * GDk;
+                }
             }
             if (MODE == MODE_DIAG && act) {
                 const int k = ch * L * S + l + L * sl;
@@ -915,7 +1009,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
             const T a0 = ldcg(cf);
             const T ga0 = r0 * gl[0];
             const T h0 = ga0 / (T(2) * a0);
-            const T tho = rv[R_TH];
+            const T tho = th;
 #pragma unroll
             for (int u = 0; u < (KM + L - 1) / L; ++u) {
                 const int m = l + u * L;
@@ -945,8 +1039,8 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
         d.gth[g] = tt;
         d.E[g] = E;
     }
-    if (valid && !act) carry_record<T, L>(d, g, l, par, rv);
-    update_body<T, L>(d, P, act, g, s, l, par, clk, rv, r0, ti, fx, fy, tt, gl, pre, fl, nz, false);
+    if (valid && !act) carry_record_staged<T, L>(d, g, l, par, own);
+    update_body<T, L>(d, P, act, g, s, l, par, clk, xi, yi, wf, th, r0, ti, fx, fy, tt, gl, pre, fl, nz, false);
 }
 
 // Phase B of the split step: displacement with parent drag + update of the
@@ -983,7 +1077,8 @@ __device__ __forceinline__ void update_warp_split(const DevPtrs<T>& d, int wg, i
 #pragma unroll
     for (int r = 0; r < NCM; ++r) gl[r] = ldcg(d.glab + (size_t)gg * NCM + r);
     const T fx = ldcg(d.gx + gg), fy = ldcg(d.gy + gg), tt = ldcg(d.gth + gg);
-    update_body<T, L>(d, P, act, g, s, l, par, clk, rv, r0, ti, fx, fy, tt, gl, pre, fl, nz, true);
+    update_body<T, L>(d, P, act, g, s, l, par, clk, rv[R_X], rv[R_Y], rv[R_W], rv[R_TH], r0, ti, fx, fy, tt, gl, pre, fl,
+                      nz, true);
 }
 
 // Last block of a step's closing barrier: tick the clocks of the simulations
@@ -1048,11 +1143,25 @@ __device__ __forceinline__ const SimDesc<T>* copy_desc(const DevPtrs<T>& d) {
     return reinterpret_cast<const SimDesc<T>*>(s_desc);
 }
 
-// Dynamic shared memory of the force kernels: one neighbour stage per warp.
+// Dynamic shared memory of the force kernels: the FP32 mode table (one
+// contour chunk of nodes), then one neighbour stage per warp.
 template <class T>
 __device__ __forceinline__ T* warp_stage(size_t bytes_per_warp) {
     extern __shared__ __align__(16) unsigned char fcc_smem[];
-    return reinterpret_cast<T*>(fcc_smem + (threadIdx.x >> 5) * bytes_per_warp);
+    return reinterpret_cast<T*>(fcc_smem + basis_table_bytes<T>() + (threadIdx.x >> 5) * bytes_per_warp);
+}
+
+// Copy the mode table of the first min(nth, BASIS_NODES) nodes into shared
+// memory (FP32 single-chunk kernels); returns it, or null when unused.
+template <class T, bool ONE>
+__device__ __forceinline__ const T* stage_basis(const DevPtrs<T>& d) {
+    extern __shared__ __align__(16) unsigned char fcc_smem[];
+    if (!(sizeof(T) == 4 && ONE)) return nullptr;
+    T* tab = reinterpret_cast<T*>(fcc_smem);
+    const int n = min(d.nth, BASIS_NODES) * KM * 4;
+    for (int u = threadIdx.x; u < n; u += blockDim.x) tab[u] = __ldg(d.basis + u);
+    __syncthreads();
+    return tab;
 }
 
 // Persistent cooperative step kernel: `nsteps` whole time steps per launch.
@@ -1067,13 +1176,14 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nthr = gridDim.x * blockDim.x;
     T* stage = warp_stage<T>(stage_bytes_per_warp<T, L>());
+    const T* tab = stage_basis<T, ONE>(d);
     const SimDesc<T>* sim0 = copy_desc(d);
     for (int st = 0; st < nsteps; ++st) {
         const int par = (par0 + st) & 1;
         if (ld_acquire(&d.sync->any_need))
             if (!rebuild_prologue(d, par, tid, nthr)) return;
         for (int wg = g0 + warp; wg < g1; wg += WPB)
-            forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage, par, sim0);
+            forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage, par, sim0, tab);
         if (SPLIT) {
             if (!grid_barrier(d.sync, [] {})) return;
             for (int wg = g0 + warp; wg < g1; wg += WPB) update_warp_split<T, L>(d, wg, par, sim0);
@@ -1090,8 +1200,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_gradients(DevPt
     const int wg = blockIdx.x * wpb + (threadIdx.x >> 5);
     const int ngroups = (d.Ntot + (32 / L) - 1) / (32 / L);
     T* stage = warp_stage<T>(stage_bytes_per_warp<T, L>());
+    const T* tab = stage_basis<T, ONE>(d);
     const SimDesc<T>* sim0 = copy_desc(d);
-    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG>(d, wg, stage, par, sim0);
+    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG>(d, wg, stage, par, sim0, tab);
 }
 
 // Stand-alone rebuild phases (update_neighbors!, and the stateless neighbour

@@ -349,6 +349,24 @@ fcc_status make_spec(const fcc_params* p, const fcc_bodies_host* b, SimSpec<T>& 
     return FCC_OK;
 }
 
+// cos(n phi_k), sin(n phi_k), n cos(n phi_k), n sin(n phi_k) for the nodes
+// phi_k = 2 pi k / nth and the modes n = 2..10, evaluated in double (the
+// reference's FourierBasis rows, src/basis.jl:35-63) and rounded to T.
+template <class T>
+std::vector<T> mode_table(int nth) {
+    std::vector<T> t((size_t)nth * KM * 4);
+    for (int k = 0; k < nth; ++k)
+        for (int m = 0; m < KM; ++m) {
+            const double n = m + 2, a = n * k * (2 * PI / nth);
+            T* e = t.data() + ((size_t)k * KM + m) * 4;
+            e[0] = (T)std::cos(a);
+            e[1] = (T)std::sin(a);
+            e[2] = (T)(n * std::cos(a));
+            e[3] = (T)(n * std::sin(a));
+        }
+    return t;
+}
+
 struct EngineBase {
     virtual ~EngineBase() = default;
     virtual fcc_status step(int64_t n, bool eager) = 0;
@@ -390,7 +408,7 @@ struct Engine final : EngineBase {
     int step_grid = 0;
     // device buffers
     DBuf<SimDesc<T>> sims;
-    DBuf<T> rec0, rec1, coef, R0, x0, y0, rmax0, cs, gx, gy, gth, glab, E, P, GR, GD, GDD, gcoef;
+    DBuf<T> rec0, rec1, coef, R0, x0, y0, rmax0, cs, basis, gx, gy, gth, glab, E, P, GR, GD, GDD, gcoef;
     DBuf<int> imgx, imgy, sim_of, nb_idx, nb_count, cellid, slot, perm, cstart, cstop, ccount, cell_sim, ch_idx,
         ch_count, bd_idx, bd_count, flags, maxcount;
     DBuf<long long> clock, builds;
@@ -451,6 +469,7 @@ struct Engine final : EngineBase {
         d.maxcount = maxcount.p;
         d.sync = sync.p;
         d.cs = cs.p;
+        d.basis = basis.p;
         d.gx = gx.p;
         d.gy = gy.p;
         d.gth = gth.p;
@@ -521,6 +540,7 @@ struct Engine final : EngineBase {
             csh[2 * k + 1] = (T)std::sin(phi);
         }
         FCC_TRY(cs.upload(csh, stream));
+        FCC_TRY(basis.upload(mode_table<T>(nth), stream));
         FCC_TRY(imgx.upload(std::vector<int>(b->imgx, b->imgx + N), stream));
         FCC_TRY(imgy.upload(std::vector<int>(b->imgy, b->imgy + N), stream));
         FCC_TRY(sim_of.alloc(n, stream));
@@ -551,8 +571,12 @@ struct Engine final : EngineBase {
 
     int variant = 0;
     const Variant& var() const { return VARIANTS[variant]; }
-    static constexpr size_t grad_stage_bytes() { return (size_t)(256 / 32) * stage_bytes_per_warp<T, LANES>(); }
-    size_t stage_bytes() const { return (size_t)(var().blk / 32) * (sizeof(T) == 4 ? var().stage32 : var().stage64); }
+    static constexpr size_t grad_stage_bytes() {
+        return basis_table_bytes<T>() + (size_t)(256 / 32) * stage_bytes_per_warp<T, LANES>();
+    }
+    size_t stage_bytes() const {
+        return basis_table_bytes<T>() + (size_t)(var().blk / 32) * (sizeof(T) == 4 ? var().stage32 : var().stage64);
+    }
     void* step_kernel() const { return (sizeof(T) == 4 ? var().f32 : var().f64)(one_chunk(), split); }
     void* grad_kernel() const {
         return nth <= LANES * SLOTS ? (void*)k_gradients<T, LANES, SLOTS, true> : (void*)k_gradients<T, LANES, SLOTS, false>;

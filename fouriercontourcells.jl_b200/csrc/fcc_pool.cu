@@ -228,7 +228,7 @@ struct Pool final : PoolBase {
     DBuf<int> flags, maxcount, slot_scr, ccount;
     DBuf<long long> clock, stop, builds;
     DBuf<GridSync> sync;
-    DBuf<T> gx, gy, gth, E, glab, cs;
+    DBuf<T> gx, gy, gth, E, glab, cs, basis;
     DBuf<MoveRange> moves;
 
     struct Slot {
@@ -285,7 +285,9 @@ struct Pool final : PoolBase {
     const Variant& var() const { return VARIANTS[variant < 0 ? 0 : variant]; }
     bool split() const { return nsplit > 0; }
     void* step_kernel() const { return (sizeof(T) == 4 ? var().f32 : var().f64)(nth <= var().L * var().S, split()); }
-    size_t stage_bytes() const { return (size_t)(var().blk / 32) * (sizeof(T) == 4 ? var().stage32 : var().stage64); }
+    size_t stage_bytes() const {
+        return basis_table_bytes<T>() + (size_t)(var().blk / 32) * (sizeof(T) == 4 ? var().stage32 : var().stage64);
+    }
 
     fcc_status init(const fcc_pool_params& q) {
         if (q.ntheta < 3) return fail(FCC_ERR_ARGUMENT, "pool: ntheta must be at least 3");
@@ -338,6 +340,7 @@ struct Pool final : PoolBase {
             csh[2 * k + 1] = (T)std::sin(phi);
         }
         FCC_TRY(cs.upload(csh, stream));
+        FCC_TRY(basis.upload(mode_table<T>(nth), stream));
         slots.assign(nslots, Slot{});
         for (int s = 0; s < nslots; ++s) stop_h[s] = 0;
         return sync_stream();
@@ -389,6 +392,7 @@ struct Pool final : PoolBase {
         d.maxcount = maxcount.p;
         d.sync = sync.p;
         d.cs = cs.p;
+        d.basis = basis.p;
         d.gx = gx.p;
         d.gy = gy.p;
         d.gth = gth.p;
