@@ -317,31 +317,55 @@ __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
 #ifndef FCC_BARRIER_SLEEP
 #define FCC_BARRIER_SLEEP 20  // ns between polls of the generation word
 #endif
+// What a block of a persistent launch knows of the barrier: the generation
+// word it last saw (bit 0 carries the released any_need flag, the rest counts
+// barriers), so neither the generation nor the rebuild flag costs a global
+// read at the next barrier or step.
+struct BarrierLocal {
+    unsigned gen;
+    int any;
+};
+
+// Read once per launch (the host may have set any_need between launches).
+__device__ __forceinline__ void barrier_start(GridSync* gs, BarrierLocal& bl) {
+    if (threadIdx.x == 0) {
+        bl.gen = ld_acquire(&gs->gen);
+        bl.any = ld_acquire(&gs->any_need);
+    }
+    __syncthreads();
+}
+
+// `last()` runs with all threads of the last block and returns (in thread 0)
+// the any_need flag to release, or -1 to keep the current one.
 template <class F>
-__device__ __forceinline__ bool grid_barrier(GridSync* gs, F&& last) {
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, BarrierLocal& bl, F&& last) {
     __shared__ int s_last, s_err;
     __syncthreads();
-    unsigned gen = 0;
     if (threadIdx.x == 0) {
-        gen = ld_acquire(&gs->gen);
         const unsigned prev = atom_add_acq_rel(&gs->count, 1u);
         s_last = (prev == gridDim.x - 1);
         s_err = 0;
     }
     __syncthreads();
     if (s_last) {
-        last();
+        int any = last();
         __syncthreads();
         if (threadIdx.x == 0) {
+            if (any < 0) any = bl.any;
             gs->count = 0;
+            gs->any_need = any;
 #if FCC_BARRIER_FENCE
             __threadfence();
 #endif
-            st_release(&gs->gen, gen + 1);  // release: the reset and the block's writes before it
+            const unsigned ng = (((bl.gen >> 1) + 1u) << 1) | (unsigned)(any != 0);
+            st_release(&gs->gen, ng);  // release: the reset and the block's writes before it
+            bl.gen = ng;
+            bl.any = any != 0;
         }
     } else if (threadIdx.x == 0) {
         long long it = 0;
-        while (ld_acquire(&gs->gen) == gen) {
+        unsigned v;
+        while ((v = ld_acquire(&gs->gen)) == bl.gen) {
             if (++it > SPIN_LIMIT) {
                 atomicExch(&gs->error, 1);
                 s_err = 1;
@@ -351,6 +375,8 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, F&& last) {
             __nanosleep(FCC_BARRIER_SLEEP);
 #endif
         }
+        bl.gen = v;
+        bl.any = (int)(v & 1u);
     }
     __syncthreads();
     return s_err == 0;

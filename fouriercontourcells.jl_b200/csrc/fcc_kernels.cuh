@@ -1081,54 +1081,62 @@ __device__ __forceinline__ void update_warp_split(const DevPtrs<T>& d, int wg, i
                       nz, true);
 }
 
+template <class T>
+__device__ __forceinline__ int book_one(const DevPtrs<T>& d, int s) {
+    int any = 0;
+    int f = ldcg(d.flags + s);
+    if ((f & F_ACTIVE) && !(f & (F_FROZEN | F_HOLD))) {
+        const long long c = ldcg(d.clock + s) + 1;
+        d.clock[s] = c;
+        if (d.stop && c >= ldcg(d.stop + s)) {
+            // step limit reached: hold; F_REBUILD stays for the host's
+            // rebuild decision when it releases the simulation
+            f = (f & ~F_NEED) | F_HOLD;
+        } else {
+            const bool need = (f & F_CONTACT) && ((f & F_REBUILD) || !(f & F_VALID) || d.sims[s].skin == T(0));
+            f &= ~(F_REBUILD | F_NEED);
+            if (need) {
+                f |= F_NEED;
+                any = 1;
+            }
+        }
+    } else {
+        f &= ~F_NEED;
+    }
+    d.flags[s] = f;
+    return any;
+}
+
 // Last block of a step's closing barrier: tick the clocks of the simulations
 // that stepped and decide the rebuilds of the next step (skin exceeded, list
-// invalid, or skin = 0: src/simulation.jl:132-142).
+// invalid, or skin = 0: src/simulation.jl:132-142).  Returns (in thread 0)
+// whether some simulation rebuilds at the next step.
 template <class T>
-__device__ void bookkeeping(const DevPtrs<T>& d) {
+__device__ int bookkeeping(const DevPtrs<T>& d) {
+    if (d.nsims == 1) return threadIdx.x == 0 ? book_one(d, 0) : 0;  // one thread, no block barrier
     __shared__ int s_any;
     if (threadIdx.x == 0) s_any = 0;
     __syncthreads();
-    for (int s = threadIdx.x; s < d.nsims; s += blockDim.x) {
-        int f = ldcg(d.flags + s);
-        if ((f & F_ACTIVE) && !(f & (F_FROZEN | F_HOLD))) {
-            const long long c = ldcg(d.clock + s) + 1;
-            d.clock[s] = c;
-            if (d.stop && c >= ldcg(d.stop + s)) {
-                // step limit reached: hold; F_REBUILD stays for the host's
-                // rebuild decision when it releases the simulation
-                f = (f & ~F_NEED) | F_HOLD;
-            } else {
-                const bool need = (f & F_CONTACT) && ((f & F_REBUILD) || !(f & F_VALID) || d.sims[s].skin == T(0));
-                f &= ~(F_REBUILD | F_NEED);
-                if (need) {
-                    f |= F_NEED;
-                    s_any = 1;
-                }
-            }
-        } else {
-            f &= ~F_NEED;
-        }
-        d.flags[s] = f;
-    }
+    for (int s = threadIdx.x; s < d.nsims; s += blockDim.x)
+        if (book_one(d, s)) s_any = 1;
     __syncthreads();
-    if (threadIdx.x == 0) d.sync->any_need = s_any;
+    return s_any;
 }
 
 // ============================================================= kernels ==
 template <class T>
-__device__ __forceinline__ bool rebuild_prologue(const DevPtrs<T>& d, int par, int tid, int nthr) {
-    auto noop = [] {};
+__device__ __forceinline__ bool rebuild_prologue(const DevPtrs<T>& d, int par, int tid, int nthr, BarrierLocal& bl) {
+    auto keep = [] { return -1; };
     phase_count(d, par, tid, nthr);
-    if (!grid_barrier(d.sync, noop)) return false;
+    if (!grid_barrier(d.sync, bl, keep)) return false;
     phase_scan(d);
-    if (!grid_barrier(d.sync, noop)) return false;
+    if (!grid_barrier(d.sync, bl, keep)) return false;
     phase_scatter(d, tid, nthr);
-    if (!grid_barrier(d.sync, noop)) return false;
+    if (!grid_barrier(d.sync, bl, keep)) return false;
     phase_sort(d, tid, nthr);
-    if (!grid_barrier(d.sync, noop)) return false;
+    if (!grid_barrier(d.sync, bl, keep)) return false;
     phase_neighbors(d, par, tid, nthr);
-    return grid_barrier(d.sync, noop);
+    return grid_barrier(d.sync, bl, keep);
 }
 
 // A single simulation's descriptor is read from shared memory (copied once per
@@ -1178,17 +1186,19 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
     T* stage = warp_stage<T>(stage_bytes_per_warp<T, L>());
     const T* tab = stage_basis<T, ONE>(d);
     const SimDesc<T>* sim0 = copy_desc(d);
+    __shared__ BarrierLocal bl;
+    barrier_start(d.sync, bl);
     for (int st = 0; st < nsteps; ++st) {
         const int par = (par0 + st) & 1;
-        if (ld_acquire(&d.sync->any_need))
-            if (!rebuild_prologue(d, par, tid, nthr)) return;
+        if (bl.any)
+            if (!rebuild_prologue(d, par, tid, nthr, bl)) return;
         for (int wg = g0 + warp; wg < g1; wg += WPB)
             forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage, par, sim0, tab);
         if (SPLIT) {
-            if (!grid_barrier(d.sync, [] {})) return;
+            if (!grid_barrier(d.sync, bl, [] { return -1; })) return;
             for (int wg = g0 + warp; wg < g1; wg += WPB) update_warp_split<T, L>(d, wg, par, sim0);
         }
-        if (!grid_barrier(d.sync, [&] { bookkeeping(d); })) return;
+        if (!grid_barrier(d.sync, bl, [&] { return bookkeeping(d); })) return;
     }
 }
 
