@@ -84,7 +84,6 @@ const double PI = 3.14159265358979323846;
 // Launch configurations of the step kernel: lanes per body L, node slots per
 // lane S (L*S >= 40 covers the nθ = 40 contour in one pass), and the minimum
 // resident 256-thread blocks per SM the register budget is cut for.
-constexpr int BLOCK = 256;
 
 template <class T, int L, int S, int BLK, int MB>
 void* step_fn(bool one, bool split) {
@@ -107,6 +106,7 @@ const Variant VARIANTS[] = {
     {16, 3, 256, 2, step_fn<float, 16, 3, 256, 2>, nullptr, stage_bytes_per_warp<float, 16>(), 0},
     {8, 5, 128, 5, step_fn<float, 8, 5, 128, 5>, nullptr, stage_bytes_per_warp<float, 8>(), 0},
     {16, 3, 128, 5, step_fn<float, 16, 3, 128, 5>, nullptr, stage_bytes_per_warp<float, 16>(), 0},
+    {8, 5, 224, 2, step_fn<float, 8, 5, 224, 2>, nullptr, stage_bytes_per_warp<float, 8>(), 0},
 };
 constexpr int NVARIANTS = sizeof(VARIANTS) / sizeof(VARIANTS[0]);
 constexpr int LANES = 8, SLOTS = 5;  // compute_gradients and the FP64 step

@@ -194,8 +194,8 @@ def test_pool_tune_leaves_no_trace():
     pa.run(100)
     pb.run(100)
     v, us = pa.tune(32)
-    assert v in (0, 3) and us > 0          # variants sharing 8 lanes x 5 node slots
-    assert pa.variant()["lanes"] == 8
+    assert v >= 0 and us > 0               # a variant sharing 8 lanes x 5 node slots
+    assert pa.variant()["lanes"] == 8 and pa.variant()["slots"] == 5
     pa.run(300)
     pb.run(300)
     for x, y in zip(sa, sb):
