@@ -90,11 +90,18 @@ __device__ __forceinline__ T* rec_cur_mut(const DevPtrs<T>& d, int par) {
 }
 
 // shared-memory vector loads of staged records
+#ifndef FCC_LDS_ASM
+#define FCC_LDS_ASM 0  // 1: explicit ld.shared (volatile asm); 0: plain vector load the compiler may schedule (measured 1.5% faster)
+#endif
 __device__ __forceinline__ float4 lds4(const float* p) {
+#if FCC_LDS_ASM
     float4 v;
     const unsigned a = (unsigned)__cvta_generic_to_shared(p);
     asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
     return v;
+#else
+    return *reinterpret_cast<const float4*>(p);
+#endif
 }
 struct Double4 {
     double x, y, z, w;
@@ -849,12 +856,16 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                         const T* nrec = snb + qq * RECW;
                         T xj, yj, rmj, wj;
                         lds_head(nrec, xj, yj, rmj, wj);
+                        const T dxc = minimum_image_fast(xi - xj, Lx, iLx);
+                        const T dyc = minimum_image_fast(yi - yj, Ly, iLy);
+                        const int wjv = unpack_w(wj);
+                        const T cAj = P.cA[(wjv >> 3) == pi ? 1 : 0][ti][wjv & 7];
                         T rr = R[0], rcs = C1[0], rsn = S1[0];
 #pragma unroll
                         for (int u = 1; u < S; ++u)
                             if (sl == u) rr = R[u], rcs = C1[u], rsn = S1[u];
-                        T dx = rr * rcs + minimum_image_fast(xi - xj, Lx, iLx);
-                        T dy = rr * rsn + minimum_image_fast(yi - yj, Ly, iLy);
+                        T dx = rr * rcs + dxc;
+                        T dy = rr * rsn + dyc;
                         if (rewrap) {
                             dx = minimum_image_fast(dx, Lx, iLx);
                             dy = minimum_image_fast(dy, Ly, iLy);
@@ -869,8 +880,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                         }
                         const T dd = radius_at(nrec, cp, sp) - dist;
                         // pair coupling of the terms (src/energies/contact.jl:267-293)
-                        const int wjv = unpack_w(wj);
-                        T gv = dd >= T(0) ? P.cA[(wjv >> 3) == pi ? 1 : 0][ti][wjv & 7] : T(0);
+                        T gv = dd >= T(0) ? cAj : T(0);
                         if (dd > T(0)) gv += P.cB[ti] * dd;
                         return gv;
                     };

@@ -308,6 +308,29 @@ def test_one_step_fp32_vs_fp64_oracle():
 
 
 # ------------------------------------------------------------ trajectories
+def test_short_fp32_trajectory_vs_fp64_oracle():
+    """Five FP32 steps of a 64 x 64 monolayer against the FP64 oracle, same
+    initial state and Philox stream.  Stated tolerance: 95% of the bodies
+    within 1e-5 in position (unwrapped) and 1e-6 in every shape
+    coefficient, all within 2e-3: a node at an Overlap near-tie can flip its
+    Heaviside contact in FP32 (a force jump J dphi R) and move its body by up
+    to ~1e-3 within a few steps; the rest differ at FP32 rounding."""
+    bodies, box = fcc.hexagonal_monolayer(64, 64, packing=0.95, maxmode=10, rng=7)
+    rng = np.random.default_rng(7)
+    bodies.coef[1:] = 0.02 * (2 * rng.random((bodies.ncoef - 1, bodies.n)) - 1)
+    bodies = as_f32_bodies(bodies)
+    kw = dict(types=(fcc.BodyType(v0=0.06, Dr=0.01, μab=0.1),), energies=(fcc.Tension(0.01), fcc.Overlap(1.0)),
+              dt=0.005, seed=7)
+    g = G(bodies, box, T=np.float32, **kw).step(5)
+    o = O(bodies, box, T=np.float64, **kw).step(5)
+    bg, bo = g.bodies, o.bodies
+    dr = np.hypot(bg.x + bg.imgx * box.Lx - bo.x - bo.imgx * box.Lx, bg.y + bg.imgy * box.Ly - bo.y - bo.imgy * box.Ly)
+    dc = np.abs(bg.coef - bo.coef).max(axis=0)
+    assert np.mean((dr < 1e-5) & (dc < 1e-6)) >= 0.95
+    assert dr.max() < 2e-3 and dc.max() < 2e-3
+    assert g.builds == o.builds
+
+
 @pytest.mark.parametrize("mode", ["step", "run"])
 def test_reference_n64_golden_on_gpu(ref_n64, mode):
     """The original C++ code's N = 64 trajectory (test/test_dynamics.jl:53-70)
