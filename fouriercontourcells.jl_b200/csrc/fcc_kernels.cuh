@@ -378,9 +378,15 @@ __host__ __device__ constexpr size_t basis_table_bytes() {
 
 // Per warp: the own records of its 32/L bodies, then NBMAX neighbour
 // records per body.
+// Per warp, last: a copy of the simulation descriptor its bodies belong to
+// (pools; a single simulation's is shared by the block).
+template <class T>
+__host__ __device__ constexpr size_t desc_slot_bytes() {
+    return (sizeof(SimDesc<T>) + 15) / 16 * 16;
+}
 template <class T, int L>
 __host__ __device__ constexpr size_t stage_bytes_per_warp() {
-    return (size_t)(32 / L) * (1 + NBMAX) * RECW * sizeof(T);
+    return (size_t)(32 / L) * (1 + NBMAX) * RECW * sizeof(T) + desc_slot_bytes<T>();
 }
 
 // Operands of the update loaded early (their latency overlaps the force
@@ -624,7 +630,7 @@ enum : int { MODE_FUSED = 0, MODE_FORCES = 1, MODE_DIAG = 2 };
 //   pullback glab = S' Gall                     src/gradients.jl:374-386
 template <class T, int L, int S, bool ONE, int MODE>
 __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stage, int par, const SimDesc<T>* sim0,
-                                            const T* tab) {
+                                            const T* tab, int& cached) {
     constexpr int BPW = 32 / L;
     constexpr unsigned FULL = 0xffffffffu;
     constexpr int CH16 = RECW * (int)sizeof(T) / 16;  // 16-byte chunks per record
@@ -644,8 +650,18 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
         const int gf = wg * BPW;
         s = gf < d.Ntot ? __ldg(d.sim_of + gf) : -1;
         if (s < 0) return;
+        if (s != cached) {  // the warp moved to another simulation: copy its descriptor
+            SimDesc<T>* wd = reinterpret_cast<SimDesc<T>*>(stage + (size_t)BPW * (1 + NBMAX) * RECW);
+            const unsigned* src = reinterpret_cast<const unsigned*>(d.sims + s);
+            unsigned* dst = reinterpret_cast<unsigned*>(wd);
+            __syncwarp();
+            for (int u = lane; u < (int)(sizeof(SimDesc<T>) / 4); u += 32) dst[u] = __ldg(src + u);
+            __syncwarp();
+            cached = s;
+        }
     }
-    const SimDesc<T>& P = sim0 ? *sim0 : d.sims[s];
+    const SimDesc<T>& P =
+        sim0 ? *sim0 : *reinterpret_cast<const SimDesc<T>*>(stage + (size_t)BPW * (1 + NBMAX) * RECW);
     const bool valid = sim0 ? g < d.Ntot : g < P.body_off + P.n;
     const int gg = valid ? g : (sim0 ? 0 : wg * BPW);
     const T* rc = rec_cur(d, par);
@@ -1198,12 +1214,13 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
     const SimDesc<T>* sim0 = copy_desc(d);
     __shared__ BarrierLocal bl;
     barrier_start(d.sync, bl);
+    int cached = -1;  // simulation whose descriptor this warp's slot holds
     for (int st = 0; st < nsteps; ++st) {
         const int par = (par0 + st) & 1;
         if (bl.any)
             if (!rebuild_prologue(d, par, tid, nthr, bl)) return;
         for (int wg = g0 + warp; wg < g1; wg += WPB)
-            forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage, par, sim0, tab);
+            forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage, par, sim0, tab, cached);
         if (SPLIT) {
             if (!grid_barrier(d.sync, bl, [] { return -1; })) return;
             for (int wg = g0 + warp; wg < g1; wg += WPB) update_warp_split<T, L>(d, wg, par, sim0);
@@ -1222,7 +1239,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_gradients(DevPt
     T* stage = warp_stage<T>(stage_bytes_per_warp<T, L>());
     const T* tab = stage_basis<T, ONE>(d);
     const SimDesc<T>* sim0 = copy_desc(d);
-    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG>(d, wg, stage, par, sim0, tab);
+    int cached = -1;
+    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG>(d, wg, stage, par, sim0, tab, cached);
 }
 
 // Stand-alone rebuild phases (update_neighbors!, and the stateless neighbour
