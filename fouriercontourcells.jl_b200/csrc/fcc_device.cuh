@@ -66,6 +66,7 @@ struct SimDesc {
     int ntypes, rewrap, has_contact, has_parent_drag, has_noise;
     int nbt, nbd;
     T v0[MT], Dr[MT], Dt[MT], mur[MT], muth[MT], muab[MT];
+    T sigr[MT], sigt[MT];  // sqrt(2 Dr dt), sqrt(2 Dt dt) in T (noise amplitudes; set with dt)
     int parent_drag[MT];
     int bt_kind[MTERM];
     uint32_t bt_mask[MTERM];

@@ -456,7 +456,7 @@ __device__ __forceinline__ void substrate_displacement(const DevPtrs<T>& d, cons
     T so, co;
     t_sincos(ldcg(rc + (size_t)c * RECW + R_TH), &so, &co);
     const T dt = P.dt;
-    const T sig = t_sqrt(T(2) * P.Dt[tc] * dt);
+    const T sig = P.sigt[tc];
     T x1 = T(0), x2 = T(0);
     if (sig != T(0)) philox_pair<T>(P.k0, P.k1, (uint32_t)(c - P.body_off + 1), (uint64_t)clk, 0u, x1, x2);
     ox = dt * (P.v0[tc] * co - P.mur[tc] * fx) + sig * x1;
@@ -482,7 +482,7 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
     const T z3 = __shfl_sync(FULL, nz[0], 0, L);
     const T xi1 = __shfl_sync(FULL, nz[0], 1, L);
     const T xi2 = __shfl_sync(FULL, nz[1], 1, L);
-    const T sig_r = t_sqrt(T(2) * P.Dr[ti] * dt);
+    const T sig_r = P.sigr[ti];
     const T thn = tho - (dt * P.muth[ti]) * tt + sig_r * z3;
     T so1, co1, sn1, cn1;
     t_sincos(tho, &so1, &co1);
@@ -564,14 +564,14 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
                 const int c = unpack_w(wo) >> 3;
                 T ux, uy;
                 substrate_displacement(d, P, rc, c, clk, ux, uy);
-                const T sig = t_sqrt(T(2) * P.Dt[ti] * dt);
+                const T sig = P.sigt[ti];
                 dxp = ux + dt * (P.v0[ti] * co1 - P.mur[ti] * fx) + sig * xi1;
                 dyp = uy + dt * (P.v0[ti] * so1 - P.mur[ti] * fy) + sig * xi2;
             } else {
                 substrate_displacement(d, P, rc, g, clk, dxp, dyp);
             }
         } else {
-            const T sig = t_sqrt(T(2) * P.Dt[ti] * dt);
+            const T sig = P.sigt[ti];
             dxp = dt * (P.v0[ti] * co1 - P.mur[ti] * fx) + sig * xi1;
             dyp = dt * (P.v0[ti] * so1 - P.mur[ti] * fy) + sig * xi2;
         }
@@ -850,6 +850,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                             const T dyc = minimum_image_fast(yi - yj, Ly, iLy);
                             const T lim = rmj + crange;
                             const T lim2 = lim * lim;
+                            unsigned m = 0;  // this neighbour's hits over the lane's node slots
 #pragma unroll
                             for (int sl = 0; sl < S; ++sl) {
                                 T dx = R[sl] * C1[sl] + dxc, dy = R[sl] * S1[sl] + dyc;
@@ -857,9 +858,9 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                                     dx = minimum_image_fast(dx, Lx, iLx);
                                     dy = minimum_image_fast(dy, Ly, iLy);
                                 }
-                                if ((vmask & (1u << sl)) && dx * dx + dy * dy <= lim2)
-                                    hm |= 1ull << ((qq - q0) * S + sl);
+                                m |= (dx * dx + dy * dy <= lim2) ? (1u << sl) : 0u;
                             }
+                            hm |= (unsigned long long)(m & vmask) << ((qq - q0) * S);
                         }
                     }
                     // (2) every lane walks its own hits in (neighbour, node) order, so

@@ -126,6 +126,17 @@ struct SimSpec {
     int ccap = 1, bcap = 1;
 };
 
+// sqrt(2 D dt) of every type, evaluated in T exactly as the device would
+// (the step reads them from the descriptor)
+template <class T>
+void set_noise_amplitudes(SimDesc<T>& s) {
+    for (int t = 0; t < MT; ++t) {
+        const T a = T(2) * s.Dr[t], b = T(2) * s.Dt[t];
+        s.sigr[t] = std::sqrt(T(a * s.dt));
+        s.sigt[t] = std::sqrt(T(b * s.dt));
+    }
+}
+
 template <class T>
 fcc_status make_spec(const fcc_params* p, const fcc_bodies_host* b, SimSpec<T>& sp) {
     // validation in the order of src/simulation.jl:66-105
@@ -240,6 +251,7 @@ fcc_status make_spec(const fcc_params* p, const fcc_bodies_host* b, SimSpec<T>& 
         s.muab[t] = (T)bt.mu_ab;
         s.parent_drag[t] = bt.parent_drag;
     }
+    set_noise_amplitudes(s);
     auto mask_of = [](const fcc_term& ft) {
         if (ft.ntypes_on == 0) return 0xffffffffu;
         uint32_t m = 0;
@@ -871,7 +883,8 @@ struct Engine final : EngineBase {
 
     fcc_status set_dt(double dt) override {
         desc.dt = (T)dt;
-        CUDA_TRY(cudaMemcpyAsync(&sims.p->dt, &desc.dt, sizeof(T), cudaMemcpyHostToDevice, stream));
+        set_noise_amplitudes(desc);
+        CUDA_TRY(cudaMemcpyAsync(sims.p, &desc, sizeof(SimDesc<T>), cudaMemcpyHostToDevice, stream));
         return sync_stream();
     }
 
