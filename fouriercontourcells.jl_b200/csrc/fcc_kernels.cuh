@@ -365,9 +365,6 @@ constexpr int NBMAX = 12;
 // the angle-addition recurrence: four floats per node and mode, a node's row
 // 36 words apart (conflict-free float4 reads for the 8 nodes a warp reads).
 constexpr int BASIS_NODES = 40;
-#ifndef FCC_HIT_PAIRS
-#define FCC_HIT_PAIRS 0  // 1: the contact walk evaluates two hits per iteration
-#endif
 #ifndef FCC_MODE_TABLE
 #define FCC_MODE_TABLE 2  // 1: synthesis reads the table, 2: pullback (measured fastest), 3: both
 #endif
@@ -384,9 +381,18 @@ template <class T>
 __host__ __device__ constexpr size_t desc_slot_bytes() {
     return (sizeof(SimDesc<T>) + 15) / 16 * 16;
 }
+#ifndef FCC_WALK_SMEM
+#define FCC_WALK_SMEM 1  // 1: the hit walk reads its node (R, cos, sin) and adds its pressure in shared memory
+#endif
+// node slots per lane of a variant with L lanes per body (one 40-node chunk)
+__host__ __device__ constexpr int slots_of(int L) { return (BASIS_NODES + L - 1) / L; }
+template <class T, int L>
+__host__ __device__ constexpr size_t walk_bytes_per_warp() {
+    return FCC_WALK_SMEM ? (size_t)32 * slots_of(L) * 4 * sizeof(T) : 0;
+}
 template <class T, int L>
 __host__ __device__ constexpr size_t stage_bytes_per_warp() {
-    return (size_t)(32 / L) * (1 + NBMAX) * RECW * sizeof(T) + desc_slot_bytes<T>();
+    return (size_t)(32 / L) * (1 + NBMAX) * RECW * sizeof(T) + desc_slot_bytes<T>() + walk_bytes_per_warp<T, L>();
 }
 
 // Operands of the update loaded early (their latency overlaps the force
@@ -826,6 +832,18 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
         T p[S];
 #pragma unroll
         for (int sl = 0; sl < S; ++sl) p[sl] = T(0);
+        // per lane and node slot (R, cos, sin, pressure) for the hit walk
+        T* wsl = stage + (size_t)BPW * (1 + NBMAX) * RECW + desc_slot_bytes<T>() / sizeof(T) + (size_t)lane * S * 4;
+        if (FCC_WALK_SMEM && S <= slots_of(L) && maxc > 0) {
+#pragma unroll
+            for (int sl = 0; sl < S; ++sl) {
+                wsl[sl * 4] = R[sl];
+                wsl[sl * 4 + 1] = C1[sl];
+                wsl[sl * 4 + 2] = S1[sl];
+                wsl[sl * 4 + 3] = T(0);
+            }
+        }
+        constexpr bool WS = FCC_WALK_SMEM && S <= slots_of(L);
         if (maxc > 0) {
             // neighbours in batches of the stage (one batch unless a list is long)
             constexpr int QB = 64 / S;  // neighbours per 64-bit hit mask
@@ -877,10 +895,16 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                         const T dyc = minimum_image_fast(yi - yj, Ly, iLy);
                         const int wjv = unpack_w(wj);
                         const T cAj = P.cA[(wjv >> 3) == pi ? 1 : 0][ti][wjv & 7];
-                        T rr = R[0], rcs = C1[0], rsn = S1[0];
+                        T rr, rcs, rsn;
+                        if constexpr (WS) {
+                            const auto e = lds4(wsl + sl * 4);
+                            rr = e.x, rcs = e.y, rsn = e.z;
+                        } else {
+                            rr = R[0], rcs = C1[0], rsn = S1[0];
 #pragma unroll
-                        for (int u = 1; u < S; ++u)
-                            if (sl == u) rr = R[u], rcs = C1[u], rsn = S1[u];
+                            for (int u = 1; u < S; ++u)
+                                if (sl == u) rr = R[u], rcs = C1[u], rsn = S1[u];
+                        }
                         T dx = rr * rcs + dxc;
                         T dy = rr * rsn + dyc;
                         if (rewrap) {
@@ -901,38 +925,24 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                         if (dd > T(0)) gv += P.cB[ti] * dd;
                         return gv;
                     };
-#if FCC_HIT_PAIRS
-                    // two hits per iteration (independent chains), added in bit order
-                    while (hm) {
-                        const int ba = __ffsll((long long)hm) - 1;
-                        hm &= hm - 1;
-                        const bool two = hm != 0;
-                        const int bb = two ? __ffsll((long long)hm) - 1 : ba;
-                        if (two) hm &= hm - 1;
-                        int sa, sb;
-                        const T ga = hit_value(ba, sa);
-                        const T gb = hit_value(bb, sb);
-#pragma unroll
-                        for (int u = 0; u < S; ++u)
-                            if (sa == u) p[u] += ga;
-                        if (two) {
-#pragma unroll
-                            for (int u = 0; u < S; ++u)
-                                if (sb == u) p[u] += gb;
-                        }
-                    }
-#else
                     while (hm) {
                         const int bit = __ffsll((long long)hm) - 1;
                         hm &= hm - 1;
                         int sl;
                         const T gv = hit_value(bit, sl);
+                        if constexpr (WS) {
+                            wsl[sl * 4 + 3] += gv;
+                        } else {
 #pragma unroll
-                        for (int u = 0; u < S; ++u)
-                            if (sl == u) p[u] += gv;
+                            for (int u = 0; u < S; ++u)
+                                if (sl == u) p[u] += gv;
+                        }
                     }
-#endif
                 }
+            }
+            if constexpr (WS) {
+#pragma unroll
+                for (int sl = 0; sl < S; ++sl) p[sl] = wsl[sl * 4 + 3];
             }
         }
         if (ONE) {
