@@ -325,43 +325,58 @@ __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
 struct BarrierLocal {
     unsigned gen;
     int any;
+    int flags;        // one simulation: its flags as of the last barrier
+    long long clock;  // one simulation: its clock, ticked by every block
+    int rebuild;      // a body of this block exceeded its skin in this step
 };
 
-// Read once per launch (the host may have set any_need between launches).
-__device__ __forceinline__ void barrier_start(GridSync* gs, BarrierLocal& bl) {
+// Generation word: bit 0 the released any_need flag, bits 1-8 the flags of a
+// lone simulation, bits 9-31 a barrier counter.
+constexpr int GEN_FLAG_BITS = 9;
+
+// Read once per launch (the host may have set flags or any_need between
+// launches).  `one`: the launch advances a single simulation.
+__device__ __forceinline__ void barrier_start(GridSync* gs, BarrierLocal& bl, bool one, const int* flags,
+                                              const long long* clock) {
     if (threadIdx.x == 0) {
         bl.gen = ld_acquire(&gs->gen);
         bl.any = ld_acquire(&gs->any_need);
+        bl.flags = one ? ld_acquire(flags) : 0;
+        bl.clock = one ? *(volatile const long long*)clock : 0;
+        bl.rebuild = 0;
     }
     __syncthreads();
 }
 
-// `last()` runs with all threads of the last block and returns (in thread 0)
-// the any_need flag to release, or -1 to keep the current one.
+// Arrival carries `bits` (summed over blocks into the upper half of the
+// counter).  `last(sum_bits)` runs with all threads of the last block and
+// returns (in thread 0) the code to release — any_need | flags << 1 — or -1
+// to keep the current one.
 template <class F>
-__device__ __forceinline__ bool grid_barrier(GridSync* gs, BarrierLocal& bl, F&& last) {
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, BarrierLocal& bl, F&& last, unsigned bits = 0) {
     __shared__ int s_last, s_err;
+    __shared__ unsigned s_bits;
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned prev = atom_add_acq_rel(&gs->count, 1u);
-        s_last = (prev == gridDim.x - 1);
+        const unsigned prev = atom_add_acq_rel(&gs->count, 1u + (bits << 16));
+        s_last = ((prev & 0xffffu) == gridDim.x - 1);
+        s_bits = (prev >> 16) + bits;
         s_err = 0;
     }
     __syncthreads();
     if (s_last) {
-        int any = last();
+        int code = last(s_bits);
         __syncthreads();
         if (threadIdx.x == 0) {
-            if (any < 0) any = bl.any;
+            if (code < 0) code = bl.any | (bl.flags << 1);
             gs->count = 0;
-            gs->any_need = any;
+            gs->any_need = code & 1;
 #if FCC_BARRIER_FENCE
             __threadfence();
 #endif
-            const unsigned ng = (((bl.gen >> 1) + 1u) << 1) | (unsigned)(any != 0);
+            const unsigned ng = (((bl.gen >> GEN_FLAG_BITS) + 1u) << GEN_FLAG_BITS) | ((unsigned)code & 0x1ffu);
             st_release(&gs->gen, ng);  // release: the reset and the block's writes before it
             bl.gen = ng;
-            bl.any = any != 0;
         }
     } else if (threadIdx.x == 0) {
         long long it = 0;
@@ -377,7 +392,10 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, BarrierLocal& bl, F&&
 #endif
         }
         bl.gen = v;
-        bl.any = (int)(v & 1u);
+    }
+    if (threadIdx.x == 0) {
+        bl.any = (int)(bl.gen & 1u);
+        bl.flags = (int)((bl.gen >> 1) & 0xffu);
     }
     __syncthreads();
     return s_err == 0;

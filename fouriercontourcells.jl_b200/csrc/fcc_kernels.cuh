@@ -478,7 +478,7 @@ template <class T, int L>
 __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T>& P, bool act, int g, int s, int l,
                                             int par, long long clk, T xo, T yo, T wo, T tho, T r0, int ti, T fx, T fy,
                                             T tt, const T (&gl)[NCM], const UpdatePre<T, L>& pre, int fl,
-                                            const T (&nz)[2], bool split) {
+                                            const T (&nz)[2], bool split, int* rbp) {
     constexpr unsigned FULL = 0xffffffffu;
     constexpr int MPL = UpdatePre<T, L>::MPL;
     const T dt = P.dt;
@@ -600,7 +600,10 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
             const T dy = minimum_image_exact(sub_rn(yw, pre.y0), P.Ly);
             const T grow = sub_rn(rmax, pre.rmax0);
             const T delta = add_rn(t_sqrt(add_rn(mul_rn(dx, dx), mul_rn(dy, dy))), grow > T(0) ? grow : T(0));
-            if (mul_rn(T(2), delta) > P.skin) atomicOr(&d.flags[s], F_REBUILD);
+            if (mul_rn(T(2), delta) > P.skin) {
+                atomicOr(&d.flags[s], F_REBUILD);
+                if (rbp) *rbp = 1;  // the block's arrival at the step barrier reports it
+            }
         }
         if (!(isfinite(xw) && isfinite(yw) && isfinite(thn) && isfinite(rmax))) atomicOr(&d.flags[s], F_NONFINITE);
     }
@@ -636,7 +639,7 @@ enum : int { MODE_FUSED = 0, MODE_FORCES = 1, MODE_DIAG = 2 };
 //   pullback glab = S' Gall                     src/gradients.jl:374-386
 template <class T, int L, int S, bool ONE, int MODE>
 __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stage, int par, const SimDesc<T>* sim0,
-                                            const T* tab, int& cached) {
+                                            const T* tab, int& cached, int* rbp) {
     constexpr int BPW = 32 / L;
     constexpr unsigned FULL = 0xffffffffu;
     constexpr int CH16 = RECW * (int)sizeof(T) / 16;  // 16-byte chunks per record
@@ -1077,13 +1080,14 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
         d.E[g] = E;
     }
     if (valid && !act) carry_record_staged<T, L>(d, g, l, par, own);
-    update_body<T, L>(d, P, act, g, s, l, par, clk, xi, yi, wf, th, r0, ti, fx, fy, tt, gl, pre, fl, nz, false);
+    update_body<T, L>(d, P, act, g, s, l, par, clk, xi, yi, wf, th, r0, ti, fx, fy, tt, gl, pre, fl, nz, false, rbp);
 }
 
 // Phase B of the split step: displacement with parent drag + update of the
 // bodies of warp group `wg`, from the forces phase A stored.
 template <class T, int L>
-__device__ __forceinline__ void update_warp_split(const DevPtrs<T>& d, int wg, int par, const SimDesc<T>* sim0) {
+__device__ __forceinline__ void update_warp_split(const DevPtrs<T>& d, int wg, int par, const SimDesc<T>* sim0,
+                                                  int* rbp) {
     constexpr int BPW = 32 / L;
     const int lane = threadIdx.x & 31;
     const int l = lane & (L - 1);
@@ -1115,7 +1119,7 @@ __device__ __forceinline__ void update_warp_split(const DevPtrs<T>& d, int wg, i
     for (int r = 0; r < NCM; ++r) gl[r] = ldcg(d.glab + (size_t)gg * NCM + r);
     const T fx = ldcg(d.gx + gg), fy = ldcg(d.gy + gg), tt = ldcg(d.gth + gg);
     update_body<T, L>(d, P, act, g, s, l, par, clk, rv[R_X], rv[R_Y], rv[R_W], rv[R_TH], r0, ti, fx, fy, tt, gl, pre, fl,
-                      nz, true);
+                      nz, true, rbp);
 }
 
 template <class T>
@@ -1144,12 +1148,40 @@ __device__ __forceinline__ int book_one(const DevPtrs<T>& d, int s) {
     return any;
 }
 
+// A launch that advances one simulation with no step limit: its flags and
+// clock are known to every block (released with each barrier, ticked
+// locally), so the bookkeeping needs no global reads.
+template <class T>
+__device__ __forceinline__ bool lone_sim(const DevPtrs<T>& d) {
+    return d.nsims == 1 && d.stop == nullptr;
+}
+
 // Last block of a step's closing barrier: tick the clocks of the simulations
 // that stepped and decide the rebuilds of the next step (skin exceeded, list
 // invalid, or skin = 0: src/simulation.jl:132-142).  Returns (in thread 0)
-// whether some simulation rebuilds at the next step.
+// the release code: whether some simulation rebuilds at the next step, and
+// for a lone simulation its new flags (<< 1).  `rebuilds`: blocks whose
+// bodies exceeded their skin in this step.
 template <class T>
-__device__ int bookkeeping(const DevPtrs<T>& d) {
+__device__ int bookkeeping(const DevPtrs<T>& d, const BarrierLocal& bl, unsigned rebuilds) {
+    if (lone_sim(d)) {
+        if (threadIdx.x != 0) return 0;
+        int f = bl.flags, need = 0;
+        if ((f & F_ACTIVE) && !(f & (F_FROZEN | F_HOLD))) {
+            d.clock[0] = bl.clock + 1;
+            need = (f & F_CONTACT) && (rebuilds != 0 || (f & F_REBUILD) || !(f & F_VALID) || d.sims[0].skin == T(0));
+            f &= ~(F_REBUILD | F_NEED);
+            atomicAnd(d.flags, ~(F_REBUILD | F_NEED));  // keeps bits other blocks set (non-finite)
+            if (need) {
+                f |= F_NEED;
+                atomicOr(d.flags, F_NEED);
+            }
+        } else {
+            f &= ~F_NEED;
+            atomicAnd(d.flags, ~F_NEED);
+        }
+        return need | ((f & 0xff) << 1);
+    }
     if (d.nsims == 1) return threadIdx.x == 0 ? book_one(d, 0) : 0;  // one thread, no block barrier
     __shared__ int s_any;
     if (threadIdx.x == 0) s_any = 0;
@@ -1163,7 +1195,8 @@ __device__ int bookkeeping(const DevPtrs<T>& d) {
 // ============================================================= kernels ==
 template <class T>
 __device__ __forceinline__ bool rebuild_prologue(const DevPtrs<T>& d, int par, int tid, int nthr, BarrierLocal& bl) {
-    auto keep = [] { return -1; };
+    // the phases set F_VALID / F_FROZEN: a lone simulation's flags are re-read
+    auto keep = [&](unsigned) { return lone_sim(d) ? (bl.any | ((ldcg(d.flags) & 0xff) << 1)) : -1; };
     phase_count(d, par, tid, nthr);
     if (!grid_barrier(d.sync, bl, keep)) return false;
     phase_scan(d);
@@ -1224,19 +1257,29 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
     const T* tab = stage_basis<T, ONE>(d);
     const SimDesc<T>* sim0 = copy_desc(d);
     __shared__ BarrierLocal bl;
-    barrier_start(d.sync, bl);
+    const bool lone = lone_sim(d);
+    barrier_start(d.sync, bl, lone, d.flags, d.clock);
     int cached = -1;  // simulation whose descriptor this warp's slot holds
     for (int st = 0; st < nsteps; ++st) {
         const int par = (par0 + st) & 1;
         if (bl.any)
             if (!rebuild_prologue(d, par, tid, nthr, bl)) return;
         for (int wg = g0 + warp; wg < g1; wg += WPB)
-            forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage, par, sim0, tab, cached);
+            forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage, par, sim0, tab, cached,
+                                                                         &bl.rebuild);
         if (SPLIT) {
-            if (!grid_barrier(d.sync, bl, [] { return -1; })) return;
-            for (int wg = g0 + warp; wg < g1; wg += WPB) update_warp_split<T, L>(d, wg, par, sim0);
+            if (!grid_barrier(d.sync, bl, [](unsigned) { return -1; })) return;
+            for (int wg = g0 + warp; wg < g1; wg += WPB) update_warp_split<T, L>(d, wg, par, sim0, &bl.rebuild);
         }
-        if (!grid_barrier(d.sync, bl, [&] { return bookkeeping(d); })) return;
+        __syncthreads();  // every warp's skin verdict is in bl.rebuild
+        const int f0 = bl.flags;
+        unsigned rb = 0;
+        if (threadIdx.x == 0) {  // reported with the arrival; cleared before the next forces phase
+            rb = bl.rebuild ? 1u : 0u;
+            bl.rebuild = 0;
+        }
+        if (!grid_barrier(d.sync, bl, [&](unsigned rbs) { return bookkeeping(d, bl, rbs); }, rb)) return;
+        if (threadIdx.x == 0 && lone && (f0 & F_ACTIVE) && !(f0 & (F_FROZEN | F_HOLD))) bl.clock += 1;
     }
 }
 
@@ -1251,7 +1294,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_gradients(DevPt
     const T* tab = stage_basis<T, ONE>(d);
     const SimDesc<T>* sim0 = copy_desc(d);
     int cached = -1;
-    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG>(d, wg, stage, par, sim0, tab, cached);
+    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG>(d, wg, stage, par, sim0, tab, cached, nullptr);
 }
 
 // Stand-alone rebuild phases (update_neighbors!, and the stateless neighbour
