@@ -569,3 +569,26 @@ def test_full_size_invariants(nx):
         close = set(close.tolist()) - {i}
         listed = set((nb.idx[:nb.count[i], i] - 1).tolist())
         assert close <= listed
+
+
+@pytest.mark.parametrize("drag", ["parent", "substrate"])
+def test_typed_bodies_full_size(drag):
+    """The cells-with-nuclei configuration (4096 cells of R0 = 1 and 4096
+    nuclei of R0 = 0.5 at packing 0.9, OnTypes tensions 0.01 / 0.05, Overlap
+    for all pairs, nuclei without self-propulsion), FP32, 200 steps: finite
+    state, areas pi R0^2 kept, shape bound, every type's shape index >= 2 sqrt(pi)."""
+    cells, box = fcc.hexagonal_monolayer(64, 64, packing=0.9, maxmode=10, rng=1234)
+    nb = fcc.with_nuclei(cells, ratio=0.5)
+    kw = dict(types=(fcc.BodyType(v0=0.06, Dr=0.01, μab=0.1), fcc.BodyType(v0=0.0, drag=drag, μab=0.1)),
+              energies=(fcc.OnTypes(fcc.Tension(0.01), 1), fcc.OnTypes(fcc.Tension(0.05), 2), fcc.Overlap(1.0)),
+              dt=0.005, seed=1234)
+    sim = G(nb, box, T=np.float32, **kw)
+    sim.run(200)
+    b = sim.bodies
+    assert b.n == 8192 and np.isfinite(b.x).all() and np.isfinite(b.coef).all()
+    assert np.allclose(fcc.areas(sim), math.pi * f32(nb.R0) ** 2, rtol=2e-5)
+    s = np.hypot(b.coef[1:10], b.coef[10:]).sum(0)
+    assert (s <= math.sqrt(2 / 3) * (1 + 1e-6)).all()
+    for t in (1, 2):
+        assert (fcc.shape_index(sim, type=t) >= 2 * math.sqrt(math.pi) * (1 - 1e-6)).all()
+    assert sim.nsteps == 200 and sim.builds >= 1
