@@ -596,13 +596,12 @@ struct Engine final : EngineBase {
 
     bool one_chunk() const { return nth <= var().L * var().S; }
 
-    // Variant choice: FCC_VARIANT overrides; FP64 always uses variant 0.
+    // Variant choice: FCC_VARIANT overrides (FP64: only variants with an FP64 build).
     void choose_variant() {
         variant = 0;
-        if (sizeof(T) != 4) return;
         if (const char* e = std::getenv("FCC_VARIANT")) {
             const int v = std::atoi(e);
-            if (v >= 0 && v < NVARIANTS) variant = v;
+            if (v >= 0 && v < NVARIANTS && (sizeof(T) == 4 || VARIANTS[v].f64)) variant = v;
         }
     }
 
