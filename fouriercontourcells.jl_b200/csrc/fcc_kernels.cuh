@@ -639,7 +639,7 @@ enum : int { MODE_FUSED = 0, MODE_FORCES = 1, MODE_DIAG = 2 };
 //   pullback glab = S' Gall                     src/gradients.jl:374-386
 template <class T, int L, int S, bool ONE, int MODE>
 __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stage, int par, const SimDesc<T>* sim0,
-                                            const T* tab, int& cached, int* rbp) {
+                                            const T* tab, int& cached, int* rbp, const BarrierLocal* lone) {
     constexpr int BPW = 32 / L;
     constexpr unsigned FULL = 0xffffffffu;
     constexpr int CH16 = RECW * (int)sizeof(T) / 16;  // 16-byte chunks per record
@@ -693,8 +693,9 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
         const int q = l + u * L;
         ids[u] = q < min(d.cap, NBMAX) ? ldcg(d.nb_idx + (size_t)gg * d.cap + q) : gg;
     }
-    const int fl = ldcg(d.flags + s);
-    const long long clk = ldcg(d.clock + s);
+    // a lone simulation's flags and clock are known to the block (released with the barrier)
+    const int fl = lone ? lone->flags : ldcg(d.flags + s);
+    const long long clk = lone ? lone->clock : ldcg(d.clock + s);
     UpdatePre<T, L> pre;
     if (MODE == MODE_FUSED) load_update_pre(d, gg, l, P.K, pre);
     bool act = valid;
@@ -1266,7 +1267,7 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
             if (!rebuild_prologue(d, par, tid, nthr, bl)) return;
         for (int wg = g0 + warp; wg < g1; wg += WPB)
             forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage, par, sim0, tab, cached,
-                                                                         &bl.rebuild);
+                                                                         &bl.rebuild, lone ? &bl : nullptr);
         if (SPLIT) {
             if (!grid_barrier(d.sync, bl, [](unsigned) { return -1; })) return;
             for (int wg = g0 + warp; wg < g1; wg += WPB) update_warp_split<T, L>(d, wg, par, sim0, &bl.rebuild);
@@ -1294,7 +1295,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_gradients(DevPt
     const T* tab = stage_basis<T, ONE>(d);
     const SimDesc<T>* sim0 = copy_desc(d);
     int cached = -1;
-    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG>(d, wg, stage, par, sim0, tab, cached, nullptr);
+    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG>(d, wg, stage, par, sim0, tab, cached, nullptr, nullptr);
 }
 
 // Stand-alone rebuild phases (update_neighbors!, and the stateless neighbour
