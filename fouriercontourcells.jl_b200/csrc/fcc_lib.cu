@@ -92,21 +92,26 @@ void* step_fn(bool one, bool split) {
     return split ? (void*)k_step<T, L, S, false, true, BLK, MB> : (void*)k_step<T, L, S, false, false, BLK, MB>;
 }
 
+// `family`: variants of one family give bit-identical trajectories (same
+// lanes x node slots, and — measured, since the compiler may fuse either
+// product of a*b + c*d differently under another register budget — the same
+// rounding); the autotuner keeps within the family unless told to reorder.
 struct Variant {
     int L, S, blk, minb;
     void* (*f32)(bool, bool);
     void* (*f64)(bool, bool);
     size_t stage32, stage64;  // shared-memory neighbour stage per warp
+    int family;
 };
 
 const Variant VARIANTS[] = {
     {8, 5, 256, 2, step_fn<float, 8, 5, 256, 2>, step_fn<double, 8, 5, 256, 1>, stage_bytes_per_warp<float, 8>(),
-     stage_bytes_per_warp<double, 8>()},
-    {4, 10, 256, 2, step_fn<float, 4, 10, 256, 2>, nullptr, stage_bytes_per_warp<float, 4>(), 0},
-    {16, 3, 256, 2, step_fn<float, 16, 3, 256, 2>, nullptr, stage_bytes_per_warp<float, 16>(), 0},
-    {8, 5, 128, 5, step_fn<float, 8, 5, 128, 5>, nullptr, stage_bytes_per_warp<float, 8>(), 0},
-    {16, 3, 128, 5, step_fn<float, 16, 3, 128, 5>, nullptr, stage_bytes_per_warp<float, 16>(), 0},
-    {8, 5, 224, 2, step_fn<float, 8, 5, 224, 2>, nullptr, stage_bytes_per_warp<float, 8>(), 0},
+     stage_bytes_per_warp<double, 8>(), 0},
+    {4, 10, 256, 2, step_fn<float, 4, 10, 256, 2>, nullptr, stage_bytes_per_warp<float, 4>(), 0, 1},
+    {16, 3, 256, 2, step_fn<float, 16, 3, 256, 2>, nullptr, stage_bytes_per_warp<float, 16>(), 0, 2},
+    {8, 5, 128, 5, step_fn<float, 8, 5, 128, 5>, nullptr, stage_bytes_per_warp<float, 8>(), 0, 3},
+    {16, 3, 128, 5, step_fn<float, 16, 3, 128, 5>, nullptr, stage_bytes_per_warp<float, 16>(), 0, 2},
+    {8, 5, 224, 2, step_fn<float, 8, 5, 224, 2>, nullptr, stage_bytes_per_warp<float, 8>(), 0, 0},
 };
 constexpr int NVARIANTS = sizeof(VARIANTS) / sizeof(VARIANTS[0]);
 constexpr int LANES = 8, SLOTS = 5;  // compute_gradients and the FP64 step

@@ -793,11 +793,11 @@ struct Pool final : PoolBase {
     // power of two, precision): each candidate variant runs `steps` steps of
     // the live pool from a snapshot, the fastest is kept, and the snapshot is
     // restored, so tuning leaves no trace in the trajectories.  By default the
-    // candidates are the variants with the current lanes x node slots (block
-    // size and register budget differ; the arithmetic and its order do not,
-    // so results stay bit-identical); `reorder` admits every variant (other
-    // lane counts sum node quadratures in another order: results then agree
-    // with the default to FP32 rounding, not bit for bit).
+    // candidates are the current variant's family (block size and register
+    // budget differ, the rounding is measured identical, so results stay
+    // bit-identical); `reorder` admits every variant (other lane counts sum
+    // node quadratures in another order: results then agree with the default
+    // to FP32 rounding, not bit for bit).
     static std::map<std::pair<int, int>, int>& tune_table() {
         static std::map<std::pair<int, int>, int> t;
         return t;
@@ -900,7 +900,7 @@ struct Pool final : PoolBase {
         for (int v = 0; v < NVARIANTS; ++v) {
             const Variant& c = VARIANTS[v];
             if (sizeof(T) != 4 && !c.f64) continue;
-            if (!reorder && (c.L != cur.L || c.S != cur.S)) continue;
+            if (!reorder && c.family != cur.family) continue;
             variant = v;
             drop_graph();
             std::vector<long long> target(nslots, 0);

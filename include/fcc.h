@@ -321,9 +321,9 @@ fcc_status fcc_pool_last_timing(fcc_pool* pool, double* ms, int64_t* launches, i
  * (tuning leaves the trajectories untouched), and keep the fastest for this
  * size bucket (packed bodies rounded up to a power of two) in a process-wide
  * table that later runs of any pool of that bucket use unless fcc_pool_config
- * fixed a variant.  reorder = 0: only variants with the current lanes x node
- * slots (results stay bit-identical); 1: every variant (node quadratures then
- * sum in another order: results agree to FP32 rounding).  *variant = -1 when
+ * fixed a variant.  reorder = 0: only variants of the current one's family
+ * (same lanes x node slots and measured identical rounding: results stay
+ * bit-identical); 1: every variant (results agree to FP32 rounding).  *variant = -1 when
  * a neighbour list would have to regrow first (nothing tuned). */
 fcc_status fcc_pool_tune(fcc_pool* pool, int64_t steps, int32_t reorder, int32_t* variant, double* us_per_step);
 

@@ -204,3 +204,21 @@ def test_pool_tune_leaves_no_trace():
         for f in ("x", "y", "θ", "coef", "imgx", "imgy"):
             assert np.array_equal(getattr(a[0], f), getattr(b[0], f)), f
         assert pa.builds(x) == pb.builds(y)
+
+
+@pytest.mark.parametrize("family", [(0, 5), (2, 4)])
+def test_variant_families_give_identical_bits(family, monkeypatch):
+    """Launch variants the library groups into one family (same lanes x node
+    slots, other block size / register budget) produce bit-identical
+    trajectories: the property the autotuner's default candidate set relies on."""
+    b, box, kw = monolayer(24, 24, 31, 0.2, 0.01, True, np.float32, fast=True)
+    out = []
+    for v in family:
+        monkeypatch.setenv("FCC_VARIANT", str(v))
+        s = fcc.Simulation(b, box, T=np.float32, **kw)
+        s.run(300)
+        out.append((s.bodies, s.builds))
+    (a, ba), (c, bc) = out
+    assert ba == bc and ba > 5
+    for f in ("x", "y", "θ", "coef", "imgx", "imgy"):
+        assert np.array_equal(getattr(a, f), getattr(c, f)), f
