@@ -307,7 +307,7 @@ def make_request(fcc, sp):
     return fcc.Request(bodies, box, kw, sp["horizon"], sp["arrival"], sp["id"])
 
 
-def serving_leg(fcc, oracle, work=1.5e10, pool_bodies=1 << 19):
+def serving_leg(fcc, oracle, work=1.5e10, pool_bodies=1 << 19, policy="fifo"):
     """The first requests of the serving stream (up to `work` body-steps),
     served by continuous batching on one pool sized from an HBM budget, then
     the same requests run one at a time (the plain loop)."""
@@ -324,7 +324,7 @@ def serving_leg(fcc, oracle, work=1.5e10, pool_bodies=1 << 19):
     reqs = [make_request(fcc, sp) for sp in sample]
     budget = fcc.Pool.device_bytes(np.float32, 40, pool_bodies, pool_bodies // 4, 256)
     pool = fcc.Pool.for_budget(budget, T=np.float32, max_sims=256)
-    srv = fcc.Server(pool, chunk=512)
+    srv = fcc.Server(pool, chunk=512, policy=policy)
     torch.cuda.synchronize()
     res = srv.serve(reqs)
     served = fcc.serving.summary(res)
@@ -353,7 +353,7 @@ def serving_leg(fcc, oracle, work=1.5e10, pool_bodies=1 << 19):
             "sample": f"the first {len(reqs)} requests of the seeded 2000-request stream ({acc:.3g} body-steps)",
             "offered_body_steps_per_s": offered,
             "pool": {"hbm_budget_bytes": budget, "max_bodies": u["max_bodies"], "max_sims": u["max_sims"]},
-            "served": served, "plain": plain,
+            "policy": policy, "served": served, "plain": plain,
             "served_over_plain": served["body_steps_per_s"] / plain["body_steps_per_s"],
             "chunks": srv.chunks, "bitwise_equal_to_alone": f"{equal}/{len(reqs)}",
             "audit_force_error_vs_fp64": errs}
@@ -495,7 +495,7 @@ def gpu_arm(args):
         achieved_tf = flops_b * N * steps_per_launch / (launch_ms * 1e-3) / 1e12
         cpu, _ = cpu_baseline(fcc, oracle)
         batched = batched_leg(fcc, steps=args.batch_steps) if not args.skip_batched else None
-        served = serving_leg(fcc, oracle, work=args.serve_work) if args.serve_work > 0 else None
+        served = serving_leg(fcc, oracle, work=args.serve_work, policy=args.serve_policy) if args.serve_work > 0 else None
         ferr = force_error(fcc, oracle, out, box, kw)
         line = {
             "metric": METRIC, "value": value, "unit": "body-steps/s", "n_gpus": world, "steps": steps,
@@ -539,6 +539,7 @@ def main():
     ap.add_argument("--serve-work", type=float, default=1.5e10,
                     help="body-steps of the serving sample (0: leave out the serving leg)")
     ap.add_argument("--batch-steps", type=int, default=2000, help="steps of the batching leg")
+    ap.add_argument("--serve-policy", default="fifo", choices=["fifo", "sjf"], help="serving admission order")
     ap.add_argument("--only", choices=["batched", "serving"],
                     help="run one leg alone and print its JSON (profiling; not the bench line)")
     args = ap.parse_args()
@@ -549,7 +550,7 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         fcc = load_package()
         out = batched_leg(fcc, steps=args.batch_steps) if args.only == "batched" else \
-            serving_leg(fcc, load_oracle(), work=args.serve_work)
+            serving_leg(fcc, load_oracle(), work=args.serve_work, policy=args.serve_policy)
         print(json.dumps({"leg": args.only, **out}, default=str), flush=True)
     else:
         gpu_arm(args)

@@ -186,6 +186,8 @@ class Pool:
     # ------------------------------------------------------------ state
     def state(self, slot: int):
         """(Bodies, clock, t, steps) of one simulation."""
+        if slot not in self._slots:
+            raise ArgumentError(f"pool: no simulation in slot {slot}")
         n, ncoef, _, _ = self._slots[slot]
         buf = abi.BodiesBuffer(n, ncoef)
         clk, t, stp = C.c_int64(), C.c_double(), C.c_int64()
@@ -196,6 +198,8 @@ class Pool:
         return self.state(slot)[0]
 
     def _observable(self, slot, which, type):
+        if slot not in self._slots:
+            raise ArgumentError(f"pool: no simulation in slot {slot}")
         n = self._slots[slot][0]
         out = np.zeros(max(1, n))
         cnt = C.c_int64()

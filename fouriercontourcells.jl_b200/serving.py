@@ -61,9 +61,17 @@ class Server:
 
     ``chunk`` caps the steps between two admission/retirement points; the loop
     shortens a chunk to the fewest steps any admitted simulation has left, so a
-    finished simulation leaves (and frees its room) at once."""
+    finished simulation leaves (and frees its room) at once.  ``policy``:
+    "fifo" admits in arrival order (a request that does not fit yet blocks the
+    ones behind it); "sjf" admits the waiting requests with the least work
+    (bodies × horizon) first and fills the room with any that fit (lower
+    median time to result under overload; large requests wait longer)."""
 
-    def __init__(self, pool, chunk=512, min_chunk=32, T=np.float32, clock=time.perf_counter, sleep=time.sleep):
+    def __init__(self, pool, chunk=512, min_chunk=32, T=np.float32, clock=time.perf_counter, sleep=time.sleep,
+                 policy="fifo"):
+        if policy not in ("fifo", "sjf"):
+            raise ArgumentError("policy must be 'fifo' or 'sjf'")
+        self.policy = policy
         self.pool = pool
         self.chunk = int(chunk)
         self.min_chunk = int(min_chunk)
@@ -92,13 +100,23 @@ class Server:
             t = now()
             while pending and pending[0].arrival <= t:
                 waiting.append(pending.popleft())
-            while waiting:  # admission in arrival order, as slots and memory free up
-                r = waiting[0]
-                slot = self.pool.try_add(r.bodies, r.box, horizon=r.horizon, **r.kw)
-                if slot is None:
-                    break
-                waiting.popleft()
-                active[slot] = (r, now())
+            if self.policy == "fifo":
+                while waiting:  # admission in arrival order, as slots and memory free up
+                    r = waiting[0]
+                    slot = self.pool.try_add(r.bodies, r.box, horizon=r.horizon, **r.kw)
+                    if slot is None:
+                        break
+                    waiting.popleft()
+                    active[slot] = (r, now())
+            else:  # smallest work first; every waiting request that fits is admitted
+                admitted = set()
+                for r in sorted(waiting, key=lambda q: (q.work, q.arrival)):
+                    slot = self.pool.try_add(r.bodies, r.box, horizon=r.horizon, **r.kw)
+                    if slot is not None:
+                        admitted.add(id(r))
+                        active[slot] = (r, now())
+                if admitted:
+                    waiting = deque(q for q in waiting if id(q) not in admitted)
             if not active:
                 if pending:
                     self.sleep(max(0.0, pending[0].arrival - now()))

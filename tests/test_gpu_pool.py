@@ -222,3 +222,42 @@ def test_variant_families_give_identical_bits(family, monkeypatch):
     assert ba == bc and ba > 5
     for f in ("x", "y", "θ", "coef", "imgx", "imgy"):
         assert np.array_equal(getattr(a, f), getattr(c, f)), f
+
+
+def test_pool_edge_cases():
+    """Empty pools, empty simulations, run(0), retiring everything, a slot
+    that is gone, and an FP64 pool with graph replay and tuning."""
+    T = np.float32
+    pool = fcc.Pool(T=T, max_bodies=1024, max_cells=4096, max_sims=4)
+    pool.run(10)                       # nothing admitted: a no-op
+    assert pool.last_timing()[2] == 0
+    b, box, kw = monolayer(5, 6, 41, T=T)
+    empty = fcc.Bodies.new([], [], [], np.zeros((19, 0)), [])
+    s0 = pool.add(empty, box, horizon=5, **kw)   # no bodies: only the clock moves
+    s1 = pool.add(b, box, horizon=7, **kw)
+    pool.run(0)
+    assert pool.slot(s1)[1] == 0
+    pool.run(100)
+    assert pool.slot(s0)[1:] == (5, 5) and pool.slot(s1)[1:] == (7, 7)
+    assert pool.state(s0)[0].n == 0
+    assert_same(pool, s1, alone(b, box, kw, T, 7))
+    pool.remove(s0)
+    pool.remove(s1)
+    assert pool.usage()["sims"] == 0 and pool.usage()["bodies"] == 0
+    with pytest.raises(fcc.ArgumentError):
+        pool.state(s1)
+    s2 = pool.add(b, box, horizon=7, **kw)      # the arena is reusable after it emptied
+    pool.run(7)
+    assert_same(pool, s2, alone(b, box, kw, T, 7))
+    # FP64: graph replay and the autotuner keep the trajectories of a lone run
+    T = np.float64
+    ms = members(T, fast=True)[:2]
+    pool = fcc.Pool(T=T, max_bodies=2048, max_cells=2048, max_sims=4)
+    slots = [pool.add(b, box, horizon=192, **kw) for b, box, kw in ms]
+    v, us = pool.tune(16)
+    assert v == 0
+    for _ in range(3):
+        pool.run(64)
+    assert pool.graph()[0] in (True, False)
+    for sl, (b, box, kw) in zip(slots, ms):
+        assert_same(pool, sl, alone(b, box, kw, T, 192))

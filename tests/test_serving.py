@@ -127,3 +127,17 @@ def test_summary_and_sequential_latencies():
     assert s["body_steps"] == 10_000
     lat = serving.sequential_latencies([0.0, 0.0, 5.0], [1.0, 2.0, 1.0])
     assert np.allclose(lat, [1.0, 3.0, 1.0])
+
+
+def test_sjf_admits_small_work_first_and_backfills():
+    clk = FakeClock()
+    pool = FakePool(clk, max_bodies=128, max_sims=8)
+    # all waiting at t = 0: r0 is big, r1 small, r2 medium; r0 does not fit
+    # beside r2 + r1, so sjf runs r1 and r2 first and r0 after they leave
+    reqs = [req(0, 8, 12, 1000, 0.0), req(1, 2, 2, 100, 0.0), req(2, 4, 4, 300, 0.0)]
+    res = fcc.Server(pool, chunk=128, clock=clk, sleep=clk.sleep, policy="sjf").serve(reqs)
+    adds = [e[1] for e in pool.log if e[0] == "add"]
+    assert adds[:2] == [1, 2] and adds[2] == 0
+    assert [r.id for r in res][-1] == 0
+    with pytest.raises(fcc.ArgumentError):
+        fcc.Server(pool, policy="lifo")
