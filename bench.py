@@ -307,7 +307,7 @@ def make_request(fcc, sp):
     return fcc.Request(bodies, box, kw, sp["horizon"], sp["arrival"], sp["id"])
 
 
-def serving_leg(fcc, oracle, work=1.5e10, pool_bodies=1 << 19, policy="fifo"):
+def serving_leg(fcc, oracle, work=1.5e10, pool_bodies=1 << 18, policy="fifo"):
     """The first requests of the serving stream (up to `work` body-steps),
     served by continuous batching on one pool sized from an HBM budget, then
     the same requests run one at a time (the plain loop)."""
@@ -495,7 +495,8 @@ def gpu_arm(args):
         achieved_tf = flops_b * N * steps_per_launch / (launch_ms * 1e-3) / 1e12
         cpu, _ = cpu_baseline(fcc, oracle)
         batched = batched_leg(fcc, steps=args.batch_steps) if not args.skip_batched else None
-        served = serving_leg(fcc, oracle, work=args.serve_work, policy=args.serve_policy) if args.serve_work > 0 else None
+        served = serving_leg(fcc, oracle, work=args.serve_work, policy=args.serve_policy,
+                             pool_bodies=args.serve_pool_bodies) if args.serve_work > 0 else None
         ferr = force_error(fcc, oracle, out, box, kw)
         line = {
             "metric": METRIC, "value": value, "unit": "body-steps/s", "n_gpus": world, "steps": steps,
@@ -540,6 +541,8 @@ def main():
                     help="body-steps of the serving sample (0: leave out the serving leg)")
     ap.add_argument("--batch-steps", type=int, default=2000, help="steps of the batching leg")
     ap.add_argument("--serve-policy", default="fifo", choices=["fifo", "sjf"], help="serving admission order")
+    ap.add_argument("--serve-pool-bodies", type=int, default=1 << 18,
+                    help="bodies the serving pool's HBM budget is sized for")
     ap.add_argument("--only", choices=["batched", "serving"],
                     help="run one leg alone and print its JSON (profiling; not the bench line)")
     args = ap.parse_args()
@@ -550,7 +553,8 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         fcc = load_package()
         out = batched_leg(fcc, steps=args.batch_steps) if args.only == "batched" else \
-            serving_leg(fcc, load_oracle(), work=args.serve_work, policy=args.serve_policy)
+            serving_leg(fcc, load_oracle(), work=args.serve_work, policy=args.serve_policy,
+                        pool_bodies=args.serve_pool_bodies)
         print(json.dumps({"leg": args.only, **out}, default=str), flush=True)
     else:
         gpu_arm(args)
