@@ -438,10 +438,18 @@ struct Engine final : EngineBase {
         GridSync sync;
     };
     Status* st_h = nullptr;
+    // state exchange with the host (set_state / get_state): one pinned host
+    // area and one device area, allocated at the first exchange and reused,
+    // so that no call after the first allocates, frees or copies pageable memory
+    void* xch_h = nullptr;
+    size_t xch_bytes = 0;
+    DBuf<T> xch_t;
+    DBuf<int> xch_w;
 
     ~Engine() override {
         if (stream) cudaStreamSynchronize(stream);
         if (st_h) cudaFreeHost(st_h);
+        if (xch_h) cudaFreeHost(xch_h);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -628,41 +636,70 @@ struct Engine final : EngineBase {
     }
 
     // Copy a host body state in and rebuild the derived geometry (k_init).
+    // Pinned host area of the state exchange, per body: 3 + NCM + RECW T values
+    // and 3 ints.  set_state stages x, y, theta, the coefficients, the w word
+    // and the image counts; get_state reads back the record, the coefficients
+    // and the image counts.
+    fcc_status exchange_area() {
+        const size_t n = (size_t)N;
+        const size_t bytes = n * ((3 + NCM + RECW) * sizeof(T) + 3 * sizeof(int));
+        if (bytes && !(xch_h && xch_bytes >= bytes)) {
+            if (xch_h) cudaFreeHost(xch_h);
+            xch_h = nullptr;
+            xch_bytes = 0;
+            CUDA_TRY(cudaMallocHost(&xch_h, bytes));
+            xch_bytes = bytes;
+        }
+        if (xch_t.n != n * (3 + NCM)) FCC_TRY(xch_t.alloc(n * (3 + NCM), stream));
+        if (xch_w.n != n) FCC_TRY(xch_w.alloc(n, stream));
+        return FCC_OK;
+    }
+    T* xch_tvals() const { return (T*)xch_h; }
+    int* xch_ints() const { return (int*)((T*)xch_h + (size_t)N * (3 + NCM + RECW)); }
+
     fcc_status load_state(const fcc_bodies_host* b, int64_t clk) {
         const size_t n = (size_t)N;
-        std::vector<T> hx(n), hy(n), hth(n), hc(n * NCM, T(0));
-        std::vector<int> w(n), so(n, 0), cellsim((size_t)ncx * ncy, 0);
+        FCC_TRY(exchange_area());
+        T* hx = xch_tvals();
+        T* hy = hx + n;
+        T* hth = hy + n;
+        T* hc = hth + n;
+        int* w = xch_ints();
+        int* ix = w + n;
+        int* iy = ix + n;
         for (size_t i = 0; i < n; ++i) {
             hx[i] = (T)b->x[i];
             hy[i] = (T)b->y[i];
             hth[i] = (T)b->theta[i];
             const double* c = b->coef + i * nc;
-            hc[i * NCM] = (T)c[0];
+            T* r = hc + i * NCM;
+            for (int m = 0; m < NCM; ++m) r[m] = T(0);
+            r[0] = (T)c[0];
             for (int m = 0; m < K; ++m) {
-                hc[i * NCM + 1 + m] = (T)c[1 + m];
-                hc[i * NCM + 1 + KM + m] = (T)c[1 + K + m];
+                r[1 + m] = (T)c[1 + m];
+                r[1 + KM + m] = (T)c[1 + K + m];
             }
             w[i] = ((parent_h[i] - 1) << 3) | (type_h[i] - 1);
+            if (b->imgx) ix[i] = b->imgx[i];
+            if (b->imgy) iy[i] = b->imgy[i];
         }
         if (clk >= 0) clock_h = clk;
-        DBuf<T> bx, by, bth, bc;
-        DBuf<int> bw;
-        FCC_TRY(bx.upload(hx, stream));
-        FCC_TRY(by.upload(hy, stream));
-        FCC_TRY(bth.upload(hth, stream));
-        FCC_TRY(bc.upload(hc, stream));
-        FCC_TRY(bw.upload(w, stream));
+        if (n) {
+            CUDA_TRY(cudaMemcpyAsync(xch_t.p, hx, n * (3 + NCM) * sizeof(T), cudaMemcpyHostToDevice, stream));
+            CUDA_TRY(cudaMemcpyAsync(xch_w.p, w, n * sizeof(int), cudaMemcpyHostToDevice, stream));
+            if (b->imgx) CUDA_TRY(cudaMemcpyAsync(imgx.p, ix, n * sizeof(int), cudaMemcpyHostToDevice, stream));
+            if (b->imgy) CUDA_TRY(cudaMemcpyAsync(imgy.p, iy, n * sizeof(int), cudaMemcpyHostToDevice, stream));
+            CUDA_TRY(cudaMemsetAsync(sim_of.p, 0, n * sizeof(int), stream));
+        }
         CUDA_TRY(cudaMemcpyAsync(clock.p, &clock_h, sizeof(long long), cudaMemcpyHostToDevice, stream));
-        if (b->imgx) CUDA_TRY(cudaMemcpyAsync(imgx.p, b->imgx, n * sizeof(int), cudaMemcpyHostToDevice, stream));
-        if (b->imgy) CUDA_TRY(cudaMemcpyAsync(imgy.p, b->imgy, n * sizeof(int), cudaMemcpyHostToDevice, stream));
-        CUDA_TRY(cudaMemcpyAsync(sim_of.p, so.data(), n * sizeof(int), cudaMemcpyHostToDevice, stream));
-        CUDA_TRY(cudaMemcpyAsync(cell_sim.p, cellsim.data(), cellsim.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(cudaMemsetAsync(cell_sim.p, 0, (size_t)ncx * ncy * sizeof(int), stream));
         const DevPtrs<T> d = ptrs();
         if (N > 0) {
             const int grid = (int)((N + 255) / 256);
-            k_init<T><<<grid, 256, 0, stream>>>(d, par(), 0, (int)N, bx.p, by.p, bth.p, bc.p);
+            const T* dx = xch_t.p;
+            k_init<T><<<grid, 256, 0, stream>>>(d, par(), 0, (int)N, dx, dx + n, dx + 2 * n, dx + 3 * n);
             CUDA_TRY(cudaGetLastError());
-            k_set_w<T><<<grid, 256, 0, stream>>>(d, par(), 0, (int)N, bw.p);
+            k_set_w<T><<<grid, 256, 0, stream>>>(d, par(), 0, (int)N, xch_w.p);
             CUDA_TRY(cudaGetLastError());
         }
         // list invalid: the next step (or update_neighbors!) rebuilds
@@ -670,7 +707,7 @@ struct Engine final : EngineBase {
         CUDA_TRY(cudaMemcpyAsync(flags.p, &f, sizeof(int), cudaMemcpyHostToDevice, stream));
         GridSync gs{0, 0, 0, has_contact ? 1 : 0};
         CUDA_TRY(cudaMemcpyAsync(sync.p, &gs, sizeof(GridSync), cudaMemcpyHostToDevice, stream));
-        return sync_stream();  // staging buffers are freed on return
+        return sync_stream();  // the exchange area is free for the next call on return
     }
 
     int par() const { return (int)(gstep & 1); }
@@ -834,7 +871,7 @@ struct Engine final : EngineBase {
     }
 
     // engine coefficient layout [a0; a_2..a_10; b_2..b_10] -> reference rows [a0; a_2..a_M; b_2..b_M]
-    void coef_out(const std::vector<T>& src, double* dst) const {
+    void coef_out(const T* src, double* dst) const {
         for (int64_t i = 0; i < N; ++i) {
             dst[(size_t)i * nc] = (double)src[(size_t)i * NCM];
             for (int m = 0; m < K; ++m) {
@@ -854,12 +891,18 @@ struct Engine final : EngineBase {
     fcc_status get_state(fcc_bodies_host* o, int64_t* clk, double* t, int64_t* stp) override {
         if (o) {
             if (o->n != N || o->ncoef != nc) return fail(FCC_ERR_DIMENSION, "state buffers do not match the simulation");
-            std::vector<T> rec, cf;
-            std::vector<int> ix, iy;
-            FCC_TRY(fetch(par() ? rec1.p : rec0.p, (size_t)N * RECW, rec));
-            FCC_TRY(fetch(coef.p, (size_t)N * NCM, cf));
-            FCC_TRY(fetch(imgx.p, (size_t)N, ix));
-            FCC_TRY(fetch(imgy.p, (size_t)N, iy));
+            const size_t n = (size_t)N;
+            FCC_TRY(exchange_area());
+            T* cf = xch_tvals();
+            T* rec = cf + n * NCM;
+            int* ix = xch_ints();
+            int* iy = ix + n;
+            if (n) {
+                CUDA_TRY(cudaMemcpyAsync(rec, par() ? rec1.p : rec0.p, n * RECW * sizeof(T), cudaMemcpyDeviceToHost, stream));
+                CUDA_TRY(cudaMemcpyAsync(cf, coef.p, n * NCM * sizeof(T), cudaMemcpyDeviceToHost, stream));
+                CUDA_TRY(cudaMemcpyAsync(ix, imgx.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+                CUDA_TRY(cudaMemcpyAsync(iy, imgy.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+            }
             FCC_TRY(sync_stream());
             for (int64_t i = 0; i < N; ++i) {
                 if (o->x) o->x[i] = (double)rec[(size_t)i * RECW + R_X];
@@ -915,7 +958,7 @@ struct Engine final : EngineBase {
             if (!dst) return FCC_OK;
             FCC_TRY(fetch(src.p, n * NCM, a));
             FCC_TRY(sync_stream());
-            coef_out(a, dst);
+            coef_out(a.data(), dst);
             return FCC_OK;
         };
         FCC_TRY(copy_nodes(GR, o->GR));
@@ -956,7 +999,7 @@ struct Engine final : EngineBase {
             if (!dst) return FCC_OK;
             FCC_TRY(fetch(src.p, n * NCM, a));
             FCC_TRY(sync_stream());
-            coef_out(a, dst);
+            coef_out(a.data(), dst);
             return FCC_OK;
         };
         FCC_TRY(coefs(lab, o->lab));
