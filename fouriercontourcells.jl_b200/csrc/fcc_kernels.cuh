@@ -16,6 +16,8 @@
 
 #pragma once
 
+#include <climits>
+
 #include "fcc_device.cuh"
 
 namespace fcc {
@@ -224,51 +226,60 @@ __device__ void phase_count(const DevPtrs<T>& d, int par, int tid, int nthr) {
 }
 
 // exclusive scan of the cell counts of each flagged simulation (one block per
-// simulation); cell c holds perm[cstart[c] .. cstop[c]).
+// simulation); cell c holds perm[cstart[c] .. cstop[c]).  The cells go in
+// chunks of SCAN_PER per thread: a thread loads its run of counts into
+// registers (independent loads), one block-wide scan of the run totals gives
+// the run's first slot, and the thread writes its run from the registers.
+constexpr int SCAN_PER = 16;
 template <class T>
 __device__ void phase_scan(const DevPtrs<T>& d) {
     __shared__ int s_warp[32];
-    __shared__ int s_carry;
     const int nw = (blockDim.x + 31) / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int s = blockIdx.x; s < d.nsims; s += gridDim.x) {
         if (!(ldcg(d.flags + s) & F_NEED)) continue;
         const SimDesc<T>& P = d.sims[s];
-        if (threadIdx.x == 0) s_carry = P.body_off;
-        __syncthreads();
-        for (int t0 = 0; t0 < P.ncells; t0 += blockDim.x) {
-            const int u = t0 + threadIdx.x;
-            const int c = P.cell_off + u;
-            const int v = u < P.ncells ? ldcg(d.ccount + c) : 0;
-            int incl = v;
+        int carry = P.body_off;
+        for (int base = 0; base < P.ncells; base += blockDim.x * SCAN_PER) {
+            const int u0 = base + threadIdx.x * SCAN_PER;
+            const int c0 = P.cell_off + u0;
+            int v[SCAN_PER];
+            int sum = 0;
+#pragma unroll
+            for (int i = 0; i < SCAN_PER; ++i) {
+                v[i] = u0 + i < P.ncells ? ldcg(d.ccount + c0 + i) : 0;
+                sum += v[i];
+            }
+            int incl = sum;
 #pragma unroll
             for (int off = 1; off < 32; off <<= 1) {
-                int o = __shfl_up_sync(0xffffffffu, incl, off);
-                if ((threadIdx.x & 31) >= off) incl += o;
+                const int o = __shfl_up_sync(0xffffffffu, incl, off);
+                if (lane >= off) incl += o;
             }
-            if ((threadIdx.x & 31) == 31) s_warp[threadIdx.x >> 5] = incl;
+            if (lane == 31) s_warp[w] = incl;
             __syncthreads();
             if (threadIdx.x < 32) {
-                int w = threadIdx.x < nw ? s_warp[threadIdx.x] : 0;
+                int t = threadIdx.x < nw ? s_warp[threadIdx.x] : 0;
 #pragma unroll
                 for (int off = 1; off < 32; off <<= 1) {
-                    int o = __shfl_up_sync(0xffffffffu, w, off);
-                    if ((int)threadIdx.x >= off) w += o;
+                    const int o = __shfl_up_sync(0xffffffffu, t, off);
+                    if ((int)threadIdx.x >= off) t += o;
                 }
-                s_warp[threadIdx.x] = w;  // inclusive over warps
+                s_warp[threadIdx.x] = t;  // inclusive over warps
             }
             __syncthreads();
-            const int carry = s_carry;
-            const int before = (threadIdx.x >> 5) ? s_warp[(threadIdx.x >> 5) - 1] : 0;
-            const int total = s_warp[nw - 1];
-            if (u < P.ncells) {
-                const int st = carry + before + incl - v;
-                d.cstart[c] = st;
-                d.cstop[c] = st + v;
-                d.ccount[c] = 0;
+            int st = carry + (w ? s_warp[w - 1] : 0) + incl - sum;
+#pragma unroll
+            for (int i = 0; i < SCAN_PER; ++i) {
+                if (u0 + i < P.ncells) {
+                    d.cstart[c0 + i] = st;
+                    st += v[i];
+                    d.cstop[c0 + i] = st;
+                    d.ccount[c0 + i] = 0;
+                }
             }
-            __syncthreads();
-            if (threadIdx.x == 0) s_carry = carry + total;
-            __syncthreads();
+            carry += s_warp[nw - 1];
+            __syncthreads();  // s_warp is rewritten by the next chunk
         }
         if (threadIdx.x == 0) {
             d.builds[s] += 1;
@@ -289,13 +300,33 @@ __device__ void phase_scatter(const DevPtrs<T>& d, int tid, int nthr) {
 }
 
 // ties of the stable sortperm! (src/neighbors.jl:86) are ordered by body
-// index: sort each cell's few bodies ascending
+// index: sort each cell's few bodies ascending.  A cell of at most SORT_REG
+// bodies is loaded into registers at once and each body is written to its
+// rank (the ids are distinct); a larger cell takes the insertion sort.
+constexpr int SORT_REG = 16;
 template <class T>
 __device__ void phase_sort(const DevPtrs<T>& d, int tid, int nthr) {
     for (int c = tid; c < d.Ctot; c += nthr) {
         const int s = __ldg(d.cell_sim + c);
         if (!(ldcg(d.flags + s) & F_NEED)) continue;
         const int a = ldcg(d.cstart + c), b = ldcg(d.cstop + c);
+        const int n = b - a;
+        if (n <= 1) continue;
+        if (n <= SORT_REG) {
+            int v[SORT_REG];
+#pragma unroll
+            for (int i = 0; i < SORT_REG; ++i) v[i] = i < n ? ldcg(d.perm + a + i) : INT_MAX;
+#pragma unroll
+            for (int i = 0; i < SORT_REG; ++i) {
+                if (i < n) {
+                    int r = 0;
+#pragma unroll
+                    for (int k = 0; k < SORT_REG; ++k) r += v[k] < v[i] ? 1 : 0;
+                    d.perm[a + r] = v[i];
+                }
+            }
+            continue;
+        }
         for (int q = a + 1; q < b; ++q) {
             const int v = ldcg(d.perm + q);
             int r = q - 1;
@@ -311,46 +342,125 @@ __device__ void phase_sort(const DevPtrs<T>& d, int tid, int nthr) {
 // neighbour list of one body: the 3x3 grid cells around it in the
 // reference's order (oy outer, ox inner), candidates in perm order, kept if
 // |ri - rj| <= rmax_i + rmax_j + range (exactly rounded like the oracle).
+// NB_LANES lanes per body: lane h reads the ranges of cells h and 8, the
+// candidates of the nine cells are numbered in list order and taken
+// NB_LANES * NB_PER at a time, NB_PER per lane (their perm entries, then
+// their records, each as independent loads), and ballot prefixes write the
+// kept ones in list order.  A body costs four dependent L2 round trips (own
+// record, cell ranges, perm, records) instead of one per candidate.  With a
+// single simulation (sim0: its descriptor in shared memory) the per-body
+// simulation and flag reads are skipped.  tid / nthr count threads; the grid
+// is whole warps.
+constexpr int NB_LANES = 8, NB_PER = 8;
 template <class T>
-__device__ void phase_neighbors(const DevPtrs<T>& d, int par, int tid, int nthr) {
-    for (int g = tid; g < d.Ntot; g += nthr) {
-        const int s = __ldg(d.sim_of + g);
-        if (s < 0 || !(ldcg(d.flags + s) & F_NEED)) continue;
-        const SimDesc<T>& P = d.sims[s];
-        const T* rc = rec_cur(d, par);
-        const T xi = ldcg(rc + (size_t)g * RECW + R_X), yi = ldcg(rc + (size_t)g * RECW + R_Y);
-        const T rmi = ldcg(rc + (size_t)g * RECW + R_RMAX);
-        const T ri = add_rn(rmi, P.nbrange);
-        int cx, cy;
-        grid_coords(P, xi, yi, cx, cy);
-        const int rx = P.ncx >= 3 ? 1 : 0, ry = P.ncy >= 3 ? 1 : 0;
+__device__ void phase_neighbors(const DevPtrs<T>& d, int par, int tid, int nthr, const SimDesc<T>* sim0) {
+    constexpr unsigned FULL = 0xffffffffu;
+    constexpr int BPW = 32 / NB_LANES, ROUND = NB_LANES * NB_PER;
+    constexpr unsigned SUBMASK = (1u << NB_LANES) - 1u;
+    const int lane = tid & 31, h = lane % NB_LANES, sub = lane / NB_LANES;
+    if (sim0 && !(ldcg(d.flags) & F_NEED)) return;  // uniform over the grid
+    const T* rc = rec_cur(d, par);
+    // the loop bound is uniform over the warp: every lane takes every shuffle
+    for (int gw = BPW * (tid >> 5); gw < d.Ntot; gw += BPW * (nthr >> 5)) {
+        const int g = gw + sub;
+        int s = 0;
+        bool act;
+        const SimDesc<T>* P = sim0;
+        if (sim0) {
+            act = g < d.Ntot;
+        } else {
+            s = g < d.Ntot ? __ldg(d.sim_of + g) : -1;
+            act = s >= 0 && (ldcg(d.flags + s) & F_NEED);
+            P = act ? d.sims + s : nullptr;
+        }
+        T xi = T(0), yi = T(0), rmi = T(0), ri = T(0);
+        int qa0 = 0, cnt0 = 0, qa8 = 0, cnt8 = 0;
+        if (act) {
+            xi = ldcg(rc + (size_t)g * RECW + R_X);
+            yi = ldcg(rc + (size_t)g * RECW + R_Y);
+            rmi = ldcg(rc + (size_t)g * RECW + R_RMAX);
+            ri = add_rn(rmi, P->nbrange);
+            int cx, cy;
+            grid_coords(*P, xi, yi, cx, cy);
+            const int rx = P->ncx >= 3 ? 1 : 0, ry = P->ncy >= 3 ? 1 : 0;
+            const int wx = 2 * rx + 1, ncell = wx * (2 * ry + 1);
+            if (h < ncell) {
+                const int oy = h / wx - ry, ox = h % wx - rx;
+                const int cell = P->cell_off + jmod(cx + ox, P->ncx) + P->ncx * jmod(cy + oy, P->ncy);
+                qa0 = ldcg(d.cstart + cell);
+                cnt0 = ldcg(d.cstop + cell) - qa0;
+            }
+            if (8 < ncell) {  // cell 8 (ox = oy = +1), read by every lane of the body
+                const int cell = P->cell_off + jmod(cx + 1, P->ncx) + P->ncx * jmod(cy + 1, P->ncy);
+                qa8 = ldcg(d.cstart + cell);
+                cnt8 = ldcg(d.cstop + cell) - qa8;
+            }
+        }
+        int incl = cnt0;
+#pragma unroll
+        for (int off = 1; off < NB_LANES; off <<= 1) {
+            const int o = __shfl_up_sync(FULL, incl, off, NB_LANES);
+            if (h >= off) incl += o;
+        }
+        const int first8 = __shfl_sync(FULL, incl, NB_LANES - 1, NB_LANES);  // cells 0..7
+        const int total = first8 + cnt8;
+        // candidate k lies in cell c with from_c <= k < from_c + cnt_c, at perm[k + shift_c]
+        int from[9], shift[9];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            from[c] = __shfl_sync(FULL, incl - cnt0, c, NB_LANES);
+            shift[c] = __shfl_sync(FULL, qa0, c, NB_LANES) - from[c];
+        }
+        from[8] = first8;
+        shift[8] = qa8 - first8;
+        int tmax = max(total, __shfl_xor_sync(FULL, total, 8));
+        tmax = max(tmax, __shfl_xor_sync(FULL, tmax, 16));
+        int* out = d.nb_idx + (size_t)(act ? g : 0) * d.cap;
         int n = 0;
-        int* out = d.nb_idx + (size_t)g * d.cap;
-        for (int oy = -ry; oy <= ry; ++oy)
-            for (int ox = -rx; ox <= rx; ++ox) {
-                const int cell = P.cell_off + jmod(cx + ox, P.ncx) + P.ncx * jmod(cy + oy, P.ncy);
-                const int qa = ldcg(d.cstart + cell), qb = ldcg(d.cstop + cell);
-                for (int q = qa; q < qb; ++q) {
-                    const int j = ldcg(d.perm + q);
-                    if (j == g) continue;
-                    const T xj = ldcg(rc + (size_t)j * RECW + R_X), yj = ldcg(rc + (size_t)j * RECW + R_Y);
-                    const T rmj = ldcg(rc + (size_t)j * RECW + R_RMAX);
-                    const T dx = minimum_image_exact(sub_rn(xi, xj), P.Lx);
-                    const T dy = minimum_image_exact(sub_rn(yi, yj), P.Ly);
-                    const T lim = add_rn(ri, rmj);
-                    if (add_rn(mul_rn(dx, dx), mul_rn(dy, dy)) <= mul_rn(lim, lim)) {
-                        ++n;
-                        if (n <= d.cap) out[n - 1] = j;
-                    }
+        for (int k0 = 0; k0 < tmax; k0 += ROUND) {
+            int j[NB_PER];
+#pragma unroll
+            for (int i = 0; i < NB_PER; ++i) {
+                const int k = k0 + NB_LANES * i + h;
+                j[i] = -1;
+                if (k < total) {
+                    int q = k + shift[0];
+#pragma unroll
+                    for (int c = 1; c < 9; ++c)
+                        if (k >= from[c]) q = k + shift[c];
+                    j[i] = ldcg(d.perm + q);
                 }
             }
-        d.nb_count[g] = n;
-        if (n > d.cap) atomicOr(&d.flags[s], F_FROZEN);
-        atomicMax(&d.maxcount[s], n);
-        if (P.skin > T(0)) {
-            d.x0[g] = xi;
-            d.y0[g] = yi;
-            d.rmax0[g] = rmi;
+            unsigned keepbits = 0;
+#pragma unroll
+            for (int i = 0; i < NB_PER; ++i) {
+                if (j[i] >= 0 && j[i] != g) {
+                    const T* rj = rc + (size_t)j[i] * RECW;
+                    const T xj = ldcg(rj + R_X), yj = ldcg(rj + R_Y), rmj = ldcg(rj + R_RMAX);
+                    const T dx = minimum_image_exact(sub_rn(xi, xj), P->Lx);
+                    const T dy = minimum_image_exact(sub_rn(yi, yj), P->Ly);
+                    const T lim = add_rn(ri, rmj);
+                    if (add_rn(mul_rn(dx, dx), mul_rn(dy, dy)) <= mul_rn(lim, lim)) keepbits |= 1u << i;
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < NB_PER; ++i) {
+                const bool keep = (keepbits >> i) & 1u;
+                const unsigned m = (__ballot_sync(FULL, keep) >> (NB_LANES * sub)) & SUBMASK;
+                const int pos = n + __popc(m & ((1u << h) - 1u));
+                if (keep && pos < d.cap) out[pos] = j[i];
+                n += __popc(m);
+            }
+        }
+        if (act && h == 0) {
+            d.nb_count[g] = n;
+            if (n > d.cap) atomicOr(&d.flags[s], F_FROZEN);
+            atomicMax(&d.maxcount[s], n);
+            if (P->skin > T(0)) {
+                d.x0[g] = xi;
+                d.y0[g] = yi;
+                d.rmax0[g] = rmi;
+            }
         }
     }
 }
@@ -1195,7 +1305,8 @@ __device__ int bookkeeping(const DevPtrs<T>& d, const BarrierLocal& bl, unsigned
 
 // ============================================================= kernels ==
 template <class T>
-__device__ __forceinline__ bool rebuild_prologue(const DevPtrs<T>& d, int par, int tid, int nthr, BarrierLocal& bl) {
+__device__ __forceinline__ bool rebuild_prologue(const DevPtrs<T>& d, int par, int tid, int nthr, BarrierLocal& bl,
+                                                 const SimDesc<T>* sim0) {
     // the phases set F_VALID / F_FROZEN: a lone simulation's flags are re-read
     auto keep = [&](unsigned) { return lone_sim(d) ? (bl.any | ((ldcg(d.flags) & 0xff) << 1)) : -1; };
     phase_count(d, par, tid, nthr);
@@ -1206,7 +1317,7 @@ __device__ __forceinline__ bool rebuild_prologue(const DevPtrs<T>& d, int par, i
     if (!grid_barrier(d.sync, bl, keep)) return false;
     phase_sort(d, tid, nthr);
     if (!grid_barrier(d.sync, bl, keep)) return false;
-    phase_neighbors(d, par, tid, nthr);
+    phase_neighbors(d, par, tid, nthr, sim0);
     return grid_barrier(d.sync, bl, keep);
 }
 
@@ -1264,7 +1375,7 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
     for (int st = 0; st < nsteps; ++st) {
         const int par = (par0 + st) & 1;
         if (bl.any)
-            if (!rebuild_prologue(d, par, tid, nthr, bl)) return;
+            if (!rebuild_prologue(d, par, tid, nthr, bl, sim0)) return;
         for (int wg = g0 + warp; wg < g1; wg += WPB)
             forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage, par, sim0, tab, cached,
                                                                          &bl.rebuild, lone ? &bl : nullptr);
@@ -1318,7 +1429,8 @@ __global__ void k_phase_sort(DevPtrs<T> d) {
 }
 template <class T>
 __global__ void k_phase_neighbors(DevPtrs<T> d, int par) {
-    if (ldcg(&d.sync->any_need)) phase_neighbors(d, par, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+    if (ldcg(&d.sync->any_need))
+        phase_neighbors<T>(d, par, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, nullptr);
 }
 
 // Skin check of the current state (skin_check_kernel!, src/neighbors.jl:188-194).

@@ -79,6 +79,10 @@ struct DBuf {
     }
 };
 
+// blocks of 256 threads for the neighbour phase (8 lanes per body), capped;
+// the phase loops over the rest
+inline int neighbor_grid(int64_t n) { return (int)std::min<int64_t>((n + 31) / 32, 148 * 64); }
+
 const double PI = 3.14159265358979323846;
 
 // Launch configurations of the step kernel: lanes per body L, node slots per
@@ -834,7 +838,7 @@ struct Engine final : EngineBase {
             k_phase_scan<T><<<1, 1024, 0, stream>>>(dd);
             k_phase_scatter<T><<<grid, 256, 0, stream>>>(dd);
             k_phase_sort<T><<<(ncx * ncy + 255) / 256, 256, 0, stream>>>(dd);
-            k_phase_neighbors<T><<<grid, 256, 0, stream>>>(dd, par());
+            k_phase_neighbors<T><<<neighbor_grid(N), 256, 0, stream>>>(dd, par());
             k_finish_rebuild<T><<<1, 256, 0, stream>>>(dd);
             CUDA_TRY(cudaGetLastError());
             FCC_TRY(read_status());
@@ -1188,7 +1192,7 @@ fcc_status build_neighbors_t(int64_t n, const double* x, const double* y, const 
     k_phase_scan<T><<<1, 1024, 0, st>>>(d);
     k_phase_scatter<T><<<grid, 256, 0, st>>>(d);
     k_phase_sort<T><<<(int)((C + 255) / 256), 256, 0, st>>>(d);
-    k_phase_neighbors<T><<<grid, 256, 0, st>>>(d, 0);
+    k_phase_neighbors<T><<<neighbor_grid(N), 256, 0, st>>>(d, 0);
     CUDA_TRY(cudaGetLastError());
     std::vector<int> a, b, cnt;
     a.resize(N);

@@ -897,6 +897,10 @@ struct Pool final : PoolBase {
         };
         int best = -1;
         double best_t = 1e300;
+        // every candidate is timed twice, in alternation, and keeps its faster
+        // time: the first launch of a kernel (lazy module loading) and clock
+        // ramps do not decide the choice
+        for (int pass = 0; pass < 2; ++pass)
         for (int v = 0; v < NVARIANTS; ++v) {
             const Variant& c = VARIANTS[v];
             if (sizeof(T) != 4 && !c.f64) continue;
