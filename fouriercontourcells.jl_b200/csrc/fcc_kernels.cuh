@@ -210,18 +210,138 @@ __device__ __forceinline__ void grid_coords(const SimDesc<T>& P, T x, T y, int& 
 // 223-242) as a stable integer counting sort.  Each phase is a grid-stride
 // loop over the bodies or cells of the simulations flagged F_NEED.
 
+// Rebuild work list of a pool: the flagged simulations in slot order, with
+// the running sums of their real bodies and of their cells.  Every block
+// builds its own copy in shared memory when a rebuild starts (the flags do
+// not change until it ends), so the phases visit the bodies and cells of the
+// rebuilding simulations only, instead of testing every body of the arena.
+struct WorkList {
+    const int* sim;   // [m]     simulation slot
+    const int* body;  // [m + 1] real bodies before entry t
+    const int* cell;  // [m + 1] cells before entry t
+    const int* boff;  // [m]     first body of the simulation
+    const int* coff;  // [m]     first cell of the simulation
+    int m;            // entries; -1: no list (the shared area is too small)
+};
+constexpr int WL_ARRAYS = 5;
+
+// entry t holding item i of a running-sum array pre (pre[0] = 0 <= i < pre[m]):
+// the largest t < m with pre[t] <= i
+__device__ __forceinline__ int wl_find(const int* pre, int m, int i) {
+    int lo = 0, hi = m - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Build the list in `area` (cap ints of shared memory no warp is using);
+// called by every thread of the block.
 template <class T>
-__device__ void phase_count(const DevPtrs<T>& d, int par, int tid, int nthr) {
+__device__ WorkList build_worklist(const DevPtrs<T>& d, int* area, int cap) {
+    __shared__ int s_scan[3][32];
+    __shared__ int s_run[3];
+    WorkList w{};
+    w.m = -1;
+    const int stride = d.nsims + 1;
+    if (WL_ARRAYS * stride > cap) return w;  // uniform over the block
+    int* ws = area;
+    int* wb = ws + stride;
+    int* wc = wb + stride;
+    int* wo = wc + stride;
+    int* wco = wo + stride;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (threadIdx.x == 0) s_run[0] = s_run[1] = s_run[2] = 0;
+    __syncthreads();
+    for (int base = 0; base < d.nsims; base += blockDim.x) {
+        const int s = base + threadIdx.x;
+        int need = 0, n = 0, nc = 0, bo = 0, co = 0;
+        if (s < d.nsims && (ldcg(d.flags + s) & F_NEED)) {
+            const SimDesc<T>& P = d.sims[s];
+            need = 1;
+            n = P.n;
+            nc = P.ncells;
+            bo = P.body_off;
+            co = P.cell_off;
+        }
+        int a = need, b = n, c = nc;  // inclusive over the warp
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int oa = __shfl_up_sync(0xffffffffu, a, off);
+            const int ob = __shfl_up_sync(0xffffffffu, b, off);
+            const int oc = __shfl_up_sync(0xffffffffu, c, off);
+            if (lane >= off) a += oa, b += ob, c += oc;
+        }
+        if (lane == 31) s_scan[0][wid] = a, s_scan[1][wid] = b, s_scan[2][wid] = c;
+        __syncthreads();
+        if (wid == 0) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                int t = lane < nw ? s_scan[k][lane] : 0;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const int o = __shfl_up_sync(0xffffffffu, t, off);
+                    if (lane >= off) t += o;
+                }
+                s_scan[k][lane] = t;  // inclusive over warps
+            }
+        }
+        __syncthreads();
+        if (need) {
+            const int e = s_run[0] + (wid ? s_scan[0][wid - 1] : 0) + a - 1;
+            ws[e] = s;
+            wb[e] = s_run[1] + (wid ? s_scan[1][wid - 1] : 0) + b - n;
+            wc[e] = s_run[2] + (wid ? s_scan[2][wid - 1] : 0) + c - nc;
+            wo[e] = bo;
+            wco[e] = co;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_run[0] += s_scan[0][nw - 1];
+            s_run[1] += s_scan[1][nw - 1];
+            s_run[2] += s_scan[2][nw - 1];
+        }
+        __syncthreads();
+    }
+    w.m = s_run[0];
+    if (threadIdx.x == 0) {
+        wb[w.m] = s_run[1];
+        wc[w.m] = s_run[2];
+    }
+    __syncthreads();
+    w.sim = ws;
+    w.body = wb;
+    w.cell = wc;
+    w.boff = wo;
+    w.coff = wco;
+    return w;
+}
+
+template <class T>
+__device__ __forceinline__ void count_body(const DevPtrs<T>& d, const SimDesc<T>& P, int par, int g) {
+    const T* r = rec_cur(d, par) + (size_t)g * RECW;
+    int cx, cy;
+    grid_coords(P, ldcg(r + R_X), ldcg(r + R_Y), cx, cy);
+    const int cell = P.cell_off + cx + P.ncx * cy;
+    d.cellid[g] = cell;
+    d.slot[g] = atomicAdd(&d.ccount[cell], 1);
+}
+
+template <class T>
+__device__ void phase_count(const DevPtrs<T>& d, int par, int tid, int nthr, const WorkList* wl) {
+    if (wl) {
+        for (int i = tid; i < wl->body[wl->m]; i += nthr) {
+            const int t = wl_find(wl->body, wl->m, i);
+            count_body(d, d.sims[wl->sim[t]], par, wl->boff[t] + (i - wl->body[t]));
+        }
+        return;
+    }
     for (int g = tid; g < d.Ntot; g += nthr) {
         const int s = __ldg(d.sim_of + g);
         if (s < 0 || !(ldcg(d.flags + s) & F_NEED)) continue;
-        const SimDesc<T>& P = d.sims[s];
-        const T* r = rec_cur(d, par) + (size_t)g * RECW;
-        int cx, cy;
-        grid_coords(P, ldcg(r + R_X), ldcg(r + R_Y), cx, cy);
-        const int cell = P.cell_off + cx + P.ncx * cy;
-        d.cellid[g] = cell;
-        d.slot[g] = atomicAdd(&d.ccount[cell], 1);
+        count_body(d, d.sims[s], par, g);
     }
 }
 
@@ -232,12 +352,14 @@ __device__ void phase_count(const DevPtrs<T>& d, int par, int tid, int nthr) {
 // the run's first slot, and the thread writes its run from the registers.
 constexpr int SCAN_PER = 16;
 template <class T>
-__device__ void phase_scan(const DevPtrs<T>& d) {
+__device__ void phase_scan(const DevPtrs<T>& d, const WorkList* wl) {
     __shared__ int s_warp[32];
     const int nw = (blockDim.x + 31) / 32;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int s = blockIdx.x; s < d.nsims; s += gridDim.x) {
-        if (!(ldcg(d.flags + s) & F_NEED)) continue;
+    const int nk = wl ? wl->m : d.nsims;
+    for (int k = blockIdx.x; k < nk; k += gridDim.x) {
+        const int s = wl ? wl->sim[k] : k;
+        if (!wl && !(ldcg(d.flags + s) & F_NEED)) continue;
         const SimDesc<T>& P = d.sims[s];
         int carry = P.body_off;
         for (int base = 0; base < P.ncells; base += blockDim.x * SCAN_PER) {
@@ -291,7 +413,15 @@ __device__ void phase_scan(const DevPtrs<T>& d) {
 }
 
 template <class T>
-__device__ void phase_scatter(const DevPtrs<T>& d, int tid, int nthr) {
+__device__ void phase_scatter(const DevPtrs<T>& d, int tid, int nthr, const WorkList* wl) {
+    if (wl) {
+        for (int i = tid; i < wl->body[wl->m]; i += nthr) {
+            const int t = wl_find(wl->body, wl->m, i);
+            const int g = wl->boff[t] + (i - wl->body[t]);
+            d.perm[ldcg(d.cstart + ldcg(d.cellid + g)) + ldcg(d.slot + g)] = g;
+        }
+        return;
+    }
     for (int g = tid; g < d.Ntot; g += nthr) {
         const int s = __ldg(d.sim_of + g);
         if (s < 0 || !(ldcg(d.flags + s) & F_NEED)) continue;
@@ -305,10 +435,17 @@ __device__ void phase_scatter(const DevPtrs<T>& d, int tid, int nthr) {
 // rank (the ids are distinct); a larger cell takes the insertion sort.
 constexpr int SORT_REG = 16;
 template <class T>
-__device__ void phase_sort(const DevPtrs<T>& d, int tid, int nthr) {
-    for (int c = tid; c < d.Ctot; c += nthr) {
-        const int s = __ldg(d.cell_sim + c);
-        if (!(ldcg(d.flags + s) & F_NEED)) continue;
+__device__ void phase_sort(const DevPtrs<T>& d, int tid, int nthr, const WorkList* wl) {
+    const int nc = wl ? wl->cell[wl->m] : d.Ctot;
+    for (int i = tid; i < nc; i += nthr) {
+        int c = i;
+        if (wl) {
+            const int t = wl_find(wl->cell, wl->m, i);
+            c = wl->coff[t] + (i - wl->cell[t]);
+        } else {
+            const int s = __ldg(d.cell_sim + c);
+            if (!(ldcg(d.flags + s) & F_NEED)) continue;
+        }
         const int a = ldcg(d.cstart + c), b = ldcg(d.cstop + c);
         const int n = b - a;
         if (n <= 1) continue;
@@ -353,7 +490,8 @@ __device__ void phase_sort(const DevPtrs<T>& d, int tid, int nthr) {
 // is whole warps.
 constexpr int NB_LANES = 8, NB_PER = 8;
 template <class T>
-__device__ void phase_neighbors(const DevPtrs<T>& d, int par, int tid, int nthr, const SimDesc<T>* sim0) {
+__device__ void phase_neighbors(const DevPtrs<T>& d, int par, int tid, int nthr, const SimDesc<T>* sim0,
+                                const WorkList* wl) {
     constexpr unsigned FULL = 0xffffffffu;
     constexpr int BPW = 32 / NB_LANES, ROUND = NB_LANES * NB_PER;
     constexpr unsigned SUBMASK = (1u << NB_LANES) - 1u;
@@ -361,13 +499,22 @@ __device__ void phase_neighbors(const DevPtrs<T>& d, int par, int tid, int nthr,
     if (sim0 && !(ldcg(d.flags) & F_NEED)) return;  // uniform over the grid
     const T* rc = rec_cur(d, par);
     // the loop bound is uniform over the warp: every lane takes every shuffle
-    for (int gw = BPW * (tid >> 5); gw < d.Ntot; gw += BPW * (nthr >> 5)) {
-        const int g = gw + sub;
+    const int nitems = wl ? wl->body[wl->m] : d.Ntot;
+    for (int gw = BPW * (tid >> 5); gw < nitems; gw += BPW * (nthr >> 5)) {
+        int g = gw + sub;
         int s = 0;
         bool act;
         const SimDesc<T>* P = sim0;
         if (sim0) {
             act = g < d.Ntot;
+        } else if (wl) {
+            act = g < nitems;
+            if (act) {
+                const int t = wl_find(wl->body, wl->m, g);
+                s = wl->sim[t];
+                g = wl->boff[t] + (g - wl->body[t]);
+                P = d.sims + s;
+            }
         } else {
             s = g < d.Ntot ? __ldg(d.sim_of + g) : -1;
             act = s >= 0 && (ldcg(d.flags + s) & F_NEED);
@@ -1306,18 +1453,22 @@ __device__ int bookkeeping(const DevPtrs<T>& d, const BarrierLocal& bl, unsigned
 // ============================================================= kernels ==
 template <class T>
 __device__ __forceinline__ bool rebuild_prologue(const DevPtrs<T>& d, int par, int tid, int nthr, BarrierLocal& bl,
-                                                 const SimDesc<T>* sim0) {
+                                                 const SimDesc<T>* sim0, int* wl_area, int wl_cap) {
     // the phases set F_VALID / F_FROZEN: a lone simulation's flags are re-read
     auto keep = [&](unsigned) { return lone_sim(d) ? (bl.any | ((ldcg(d.flags) & 0xff) << 1)) : -1; };
-    phase_count(d, par, tid, nthr);
+    WorkList wl{};
+    wl.m = -1;
+    if (!sim0) wl = build_worklist(d, wl_area, wl_cap);
+    const WorkList* wlp = wl.m >= 0 ? &wl : nullptr;
+    phase_count(d, par, tid, nthr, wlp);
     if (!grid_barrier(d.sync, bl, keep)) return false;
-    phase_scan(d);
+    phase_scan(d, wlp);
     if (!grid_barrier(d.sync, bl, keep)) return false;
-    phase_scatter(d, tid, nthr);
+    phase_scatter(d, tid, nthr, wlp);
     if (!grid_barrier(d.sync, bl, keep)) return false;
-    phase_sort(d, tid, nthr);
+    phase_sort(d, tid, nthr, wlp);
     if (!grid_barrier(d.sync, bl, keep)) return false;
-    phase_neighbors(d, par, tid, nthr, sim0);
+    phase_neighbors(d, par, tid, nthr, sim0, wlp);
     return grid_barrier(d.sync, bl, keep);
 }
 
@@ -1339,6 +1490,12 @@ template <class T>
 __device__ __forceinline__ T* warp_stage(size_t bytes_per_warp) {
     extern __shared__ __align__(16) unsigned char fcc_smem[];
     return reinterpret_cast<T*>(fcc_smem + basis_table_bytes<T>() + (threadIdx.x >> 5) * bytes_per_warp);
+}
+// the whole stage area of the block (every warp's stage, in order)
+template <class T>
+__device__ __forceinline__ unsigned char* block_stage_of() {
+    extern __shared__ __align__(16) unsigned char fcc_smem[];
+    return fcc_smem + basis_table_bytes<T>();
 }
 
 // Copy the mode table of the first min(nth, BASIS_NODES) nodes into shared
@@ -1374,8 +1531,14 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
     int cached = -1;  // simulation whose descriptor this warp's slot holds
     for (int st = 0; st < nsteps; ++st) {
         const int par = (par0 + st) & 1;
-        if (bl.any)
-            if (!rebuild_prologue(d, par, tid, nthr, bl, sim0)) return;
+        if (bl.any) {
+            // the work list of a pool lives in the warps' stage area, free
+            // between the closing barrier of a step and the forces
+            if (!rebuild_prologue(d, par, tid, nthr, bl, sim0, reinterpret_cast<int*>(block_stage_of<T>()),
+                                  (int)(WPB * stage_bytes_per_warp<T, L>() / sizeof(int))))
+                return;
+            cached = -1;  // the descriptor slots were overwritten
+        }
         for (int wg = g0 + warp; wg < g1; wg += WPB)
             forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage, par, sim0, tab, cached,
                                                                          &bl.rebuild, lone ? &bl : nullptr);
@@ -1413,24 +1576,27 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_gradients(DevPt
 // build), one launch per phase.
 template <class T>
 __global__ void k_phase_count(DevPtrs<T> d, int par) {
-    if (ldcg(&d.sync->any_need)) phase_count(d, par, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+    if (ldcg(&d.sync->any_need))
+        phase_count<T>(d, par, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, nullptr);
 }
 template <class T>
 __global__ void k_phase_scan(DevPtrs<T> d) {
-    if (ldcg(&d.sync->any_need)) phase_scan(d);
+    if (ldcg(&d.sync->any_need)) phase_scan<T>(d, nullptr);
 }
 template <class T>
 __global__ void k_phase_scatter(DevPtrs<T> d) {
-    if (ldcg(&d.sync->any_need)) phase_scatter(d, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+    if (ldcg(&d.sync->any_need))
+        phase_scatter<T>(d, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, nullptr);
 }
 template <class T>
 __global__ void k_phase_sort(DevPtrs<T> d) {
-    if (ldcg(&d.sync->any_need)) phase_sort(d, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+    if (ldcg(&d.sync->any_need))
+        phase_sort<T>(d, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, nullptr);
 }
 template <class T>
 __global__ void k_phase_neighbors(DevPtrs<T> d, int par) {
     if (ldcg(&d.sync->any_need))
-        phase_neighbors<T>(d, par, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, nullptr);
+        phase_neighbors<T>(d, par, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, nullptr, nullptr);
 }
 
 // Skin check of the current state (skin_check_kernel!, src/neighbors.jl:188-194).
