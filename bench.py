@@ -437,6 +437,7 @@ def gpu_arm(args):
 
     # warm-up (also builds the neighbour list and settles the rebuild cadence)
     sim.run(max(3, args.warmup))
+    start, start_clock = sim.bodies, sim.clock  # the e2e runs replay the timed steps from here
     flush_l2()
     if dist:
         dist.barrier()
@@ -450,8 +451,10 @@ def gpu_arm(args):
     ms_max = max_over_ranks(ms, dist, "cuda")
     value = job_throughput(world, N, steps, ms_max * 1e-3)
 
-    # end to end through the C ABI with host buffers (wall clock, max over ranks)
-    host = sim.bodies
+    # end to end through the C ABI with host buffers (wall clock, max over
+    # ranks): the same K steps from the same state and clock (the contact work
+    # of a monolayer grows as its shapes deform, so later steps cost more)
+    host = start
     h2d = sum(getattr(host, f).nbytes for f in ("x", "y", "θ", "imgx", "imgy", "coef"))
     d2h = sum(getattr(host, f).nbytes for f in ("x", "y", "θ", "imgx", "imgy", "coef", "R0", "type", "parent"))
     # three repetitions, the median reported (a single wall-clock sample
@@ -462,7 +465,7 @@ def gpu_arm(args):
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        sim.set_state(host)
+        sim.set_state(host, clock=start_clock)
         sim.run(args.steps)
         out = sim.bodies
         e2e_runs.append(max_over_ranks(time.perf_counter() - t0, dist, "cuda"))

@@ -66,6 +66,26 @@ def test_pool_equals_alone_bitwise(T):
     assert not np.array_equal(pool.bodies(slots[0]).x[:10], pool.bodies(slots[1]).x[:10])
 
 
+@pytest.mark.parametrize("variant", [0, 3])
+def test_pool_with_many_slots_takes_the_full_scan_rebuild(variant, monkeypatch):
+    """A rebuild visits the bodies and cells of the rebuilding simulations
+    through a work list in shared memory; with more slots than that list can
+    hold (4000 here) every phase scans the whole arena instead.  Both give
+    the trajectory of the simulation alone with the same launch variant, bit
+    for bit."""
+    ms = members(np.float32, fast=True)
+    pool = fcc.Pool(T=np.float32, max_bodies=4096, max_cells=4096, max_sims=4000)
+    pool.config(variant=variant)
+    slots = [pool.add(b, box, horizon=200, **kw) for b, box, kw in ms]
+    pool.run(200)
+    assert pool.variant()["variant"] == variant
+    monkeypatch.setenv("FCC_VARIANT", str(variant))
+    for s, (b, box, kw) in zip(slots, ms):
+        ref = alone(b, box, kw, np.float32, 200)
+        assert ref.builds > 3
+        assert_same(pool, s, ref)
+
+
 def test_pool_admission_retirement_and_horizons():
     """Retire one simulation mid-run, admit another while the rest keep their
     state; every simulation stops at its own horizon."""
