@@ -618,7 +618,7 @@ __device__ void phase_neighbors(const DevPtrs<T>& d, int par, int tid, int nthr,
 constexpr int NBMAX = 12;
 
 #ifndef FCC_DYN
-#define FCC_DYN 1  // 1: single-simulation kernels: warps take their block's warp groups dynamically
+#define FCC_DYN 1  // 1: FP32, one simulation: warps take their block's warp groups dynamically
 #endif
 
 // FP32 single-chunk kernels read cos(n phi_k), sin(n phi_k) (and n times
@@ -1533,12 +1533,14 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
     const bool lone = lone_sim(d);
     barrier_start(d.sync, bl, lone, d.flags, d.clock);
     int cached = -1;  // simulation whose descriptor this warp's slot holds
-    // single-simulation kernels balance the warp groups of a block dynamically
-    // (measured: 1% faster at N = 16384; the pool kernels keep the static
-    // assignment, which spills less and was 2% faster there)
-    constexpr bool DYN = ONE && FCC_DYN;
+    // FP32 with a single simulation: the warps of a block take its warp groups
+    // dynamically (measured: 1% faster at N = 16384).  Pools keep the static
+    // assignment (2% faster there: a warp that moves to another simulation's
+    // group re-copies the descriptor), and so does FP64 (one block of 8 warps
+    // per SM: 3% faster static).
+    const bool dyn = FCC_DYN && sizeof(T) == 4 && sim0 != nullptr;
     __shared__ int s_next[2];  // next untaken warp group of the block, per step parity
-    if (DYN && threadIdx.x == 0) s_next[0] = g0 + WPB;
+    if (dyn && threadIdx.x == 0) s_next[0] = g0 + WPB;
     __syncthreads();
     for (int st = 0; st < nsteps; ++st) {
         const int par = (par0 + st) & 1;
@@ -1550,7 +1552,7 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
                 return;
             cached = -1;  // the descriptor slots were overwritten
         }
-        if (DYN) {
+        if (dyn) {
             // a warp's first group is its own; after that it takes the block's
             // next untaken group (groups cost unequal time: contacts, hits)
             if (threadIdx.x == 0) s_next[(st + 1) & 1] = g0 + WPB;  // last used by the previous step
