@@ -522,10 +522,14 @@ def gpu_arm(args):
         sm_mhz = cs["sm_mhz"] or 1965.0
         fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
         achieved_tf = flops_b * N * steps_per_launch / (launch_ms * 1e-3) / 1e12
-        cpu, _ = cpu_baseline(fcc, oracle)
-        batched = batched_leg(fcc, steps=args.batch_steps) if not args.skip_batched else None
+        # the CPU baseline and the batching and serving legs are one-GPU figures:
+        # they run at N = 1 only (the other ranks would wait for rank 0 at the
+        # closing barrier for minutes)
+        single = world == 1
+        cpu = cpu_baseline(fcc, oracle)[0] if single else None
+        batched = batched_leg(fcc, steps=args.batch_steps) if single and not args.skip_batched else None
         served = serving_leg(fcc, oracle, work=args.serve_work, policy=args.serve_policy,
-                             pool_bodies=args.serve_pool_bodies) if args.serve_work > 0 else None
+                             pool_bodies=args.serve_pool_bodies) if single and args.serve_work > 0 else None
         ferr = force_error(fcc, oracle, out, box, kw)
         line = {
             "metric": METRIC, "value": value, "unit": "body-steps/s", "n_gpus": world, "steps": steps,
