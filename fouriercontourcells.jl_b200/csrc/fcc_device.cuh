@@ -78,10 +78,11 @@ struct SimDesc {
 };
 
 struct GridSync {
-    unsigned count;
+    unsigned count;   // arrivals at even-numbered barriers
     unsigned gen;
-    int error;      // 1: a barrier wait ran out (the kernel returned early)
-    int any_need;   // some simulation rebuilds its neighbour list this step
+    int error;        // 1: a barrier wait ran out (the kernel returned early)
+    int any_need;     // some simulation rebuilds its neighbour list this step
+    unsigned count2;  // arrivals at odd-numbered barriers
 };
 
 template <class T>
@@ -291,6 +292,11 @@ __device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.w
 // others.  Waits are bounded: after SPIN_LIMIT polls a waiting block records
 // sync->error and the kernel returns (the host reports FCC_ERR_DEVICE)
 // instead of hanging.
+// Barriers alternate between two arrival counters by the parity of their
+// number; the last block clears the counter just used after its release
+// store, off the critical path: that counter is used again two barriers
+// later, and the clear precedes the block's own next arrival (an acq_rel
+// atomic), which every later barrier's release follows.
 constexpr long long SPIN_LIMIT = 1ll << 22;  // ~0.1-4 s with the back-off below
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
@@ -352,13 +358,20 @@ __device__ __forceinline__ void barrier_start(GridSync* gs, BarrierLocal& bl, bo
 // counter).  `last(sum_bits)` runs with all threads of the last block and
 // returns (in thread 0) the code to release — any_need | flags << 1 — or -1
 // to keep the current one.
-template <class F>
-__device__ __forceinline__ bool grid_barrier(GridSync* gs, BarrierLocal& bl, F&& last, unsigned bits = 0) {
+struct NoAfter {
+    __device__ void operator()(int) const {}
+};
+// `after(code)` runs in thread 0 of the last block right after the release
+// (writes that no block reads before the next barrier).
+template <class F, class A = NoAfter>
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, BarrierLocal& bl, F&& last, unsigned bits = 0,
+                                             A&& after = A{}) {
     __shared__ int s_last, s_err;
     __shared__ unsigned s_bits;
+    unsigned* cnt = ((bl.gen >> GEN_FLAG_BITS) & 1u) ? &gs->count2 : &gs->count;
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned prev = atom_add_acq_rel(&gs->count, 1u + (bits << 16));
+        const unsigned prev = atom_add_acq_rel(cnt, 1u + (bits << 16));
         s_last = ((prev & 0xffffu) == gridDim.x - 1);
         s_bits = (prev >> 16) + bits;
         s_err = 0;
@@ -369,13 +382,14 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, BarrierLocal& bl, F&&
         __syncthreads();
         if (threadIdx.x == 0) {
             if (code < 0) code = bl.any | (bl.flags << 1);
-            gs->count = 0;
-            gs->any_need = code & 1;
 #if FCC_BARRIER_FENCE
             __threadfence();
 #endif
             const unsigned ng = (((bl.gen >> GEN_FLAG_BITS) + 1u) << GEN_FLAG_BITS) | ((unsigned)code & 0x1ffu);
-            st_release(&gs->gen, ng);  // release: the reset and the block's writes before it
+            st_release(&gs->gen, ng);  // release: the block's writes before it
+            *cnt = 0;
+            gs->any_need = code & 1;   // for the host and the stand-alone kernels
+            after(code);
             bl.gen = ng;
         }
     } else if (threadIdx.x == 0) {

@@ -329,8 +329,11 @@ __device__ __forceinline__ void count_body(const DevPtrs<T>& d, const SimDesc<T>
     d.slot[g] = atomicAdd(&d.ccount[cell], 1);
 }
 
+// `lone_need`: a single simulation's rebuild decision as the block knows it
+// (the global flags may still be in flight from the last barrier), or -1:
+// read each simulation's flags.
 template <class T>
-__device__ void phase_count(const DevPtrs<T>& d, int par, int tid, int nthr, const WorkList* wl) {
+__device__ void phase_count(const DevPtrs<T>& d, int par, int tid, int nthr, const WorkList* wl, int lone_need = -1) {
     if (wl) {
         for (int i = tid; i < wl->body[wl->m]; i += nthr) {
             const int t = wl_find(wl->body, wl->m, i);
@@ -338,9 +341,10 @@ __device__ void phase_count(const DevPtrs<T>& d, int par, int tid, int nthr, con
         }
         return;
     }
+    if (lone_need == 0) return;
     for (int g = tid; g < d.Ntot; g += nthr) {
         const int s = __ldg(d.sim_of + g);
-        if (s < 0 || !(ldcg(d.flags + s) & F_NEED)) continue;
+        if (s < 0 || !(lone_need > 0 || (ldcg(d.flags + s) & F_NEED))) continue;
         count_body(d, d.sims[s], par, g);
     }
 }
@@ -1424,23 +1428,20 @@ __device__ __forceinline__ bool lone_sim(const DevPtrs<T>& d) {
 // the release code: whether some simulation rebuilds at the next step, and
 // for a lone simulation its new flags (<< 1).  `rebuilds`: blocks whose
 // bodies exceeded their skin in this step.
+// A lone simulation's decision needs no global memory (its flags are in the
+// barrier word, its descriptor `P` in shared memory); its global flags and
+// clock are written after the release (lone_book_writes).
 template <class T>
-__device__ int bookkeeping(const DevPtrs<T>& d, const BarrierLocal& bl, unsigned rebuilds) {
+__device__ int bookkeeping(const DevPtrs<T>& d, const BarrierLocal& bl, unsigned rebuilds, const SimDesc<T>* P) {
     if (lone_sim(d)) {
         if (threadIdx.x != 0) return 0;
         int f = bl.flags, need = 0;
         if ((f & F_ACTIVE) && !(f & (F_FROZEN | F_HOLD))) {
-            d.clock[0] = bl.clock + 1;
-            need = (f & F_CONTACT) && (rebuilds != 0 || (f & F_REBUILD) || !(f & F_VALID) || d.sims[0].skin == T(0));
+            need = (f & F_CONTACT) && (rebuilds != 0 || (f & F_REBUILD) || !(f & F_VALID) || P->skin == T(0));
             f &= ~(F_REBUILD | F_NEED);
-            atomicAnd(d.flags, ~(F_REBUILD | F_NEED));  // keeps bits other blocks set (non-finite)
-            if (need) {
-                f |= F_NEED;
-                atomicOr(d.flags, F_NEED);
-            }
+            if (need) f |= F_NEED;
         } else {
             f &= ~F_NEED;
-            atomicAnd(d.flags, ~F_NEED);
         }
         return need | ((f & 0xff) << 1);
     }
@@ -1454,6 +1455,23 @@ __device__ int bookkeeping(const DevPtrs<T>& d, const BarrierLocal& bl, unsigned
     return s_any;
 }
 
+// The global side of a lone simulation's bookkeeping, after the release: the
+// host reads the clock and flags after the launch, the rebuild phases read
+// F_NEED only after the first rebuild barrier (phase_count takes the decision
+// from the barrier word).  The flag updates are atomic: they keep the bits
+// other blocks set (non-finite, overflow).
+template <class T>
+__device__ __forceinline__ void lone_book_writes(const DevPtrs<T>& d, const BarrierLocal& bl, int code) {
+    const int f = bl.flags;
+    if ((f & F_ACTIVE) && !(f & (F_FROZEN | F_HOLD))) {
+        d.clock[0] = bl.clock + 1;
+        atomicAnd(d.flags, ~(F_REBUILD | F_NEED));
+        if (code & 1) atomicOr(d.flags, F_NEED);
+    } else {
+        atomicAnd(d.flags, ~F_NEED);
+    }
+}
+
 // ============================================================= kernels ==
 template <class T>
 __device__ __forceinline__ bool rebuild_prologue(const DevPtrs<T>& d, int par, int tid, int nthr, BarrierLocal& bl,
@@ -1464,7 +1482,7 @@ __device__ __forceinline__ bool rebuild_prologue(const DevPtrs<T>& d, int par, i
     wl.m = -1;
     if (!sim0) wl = build_worklist(d, wl_area, wl_cap);
     const WorkList* wlp = wl.m >= 0 ? &wl : nullptr;
-    phase_count(d, par, tid, nthr, wlp);
+    phase_count(d, par, tid, nthr, wlp, lone_sim(d) ? bl.any : -1);
     if (!grid_barrier(d.sync, bl, keep)) return false;
     phase_scan(d, wlp);
     if (!grid_barrier(d.sync, bl, keep)) return false;
@@ -1579,7 +1597,12 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
             rb = bl.rebuild ? 1u : 0u;
             bl.rebuild = 0;
         }
-        if (!grid_barrier(d.sync, bl, [&](unsigned rbs) { return bookkeeping(d, bl, rbs); }, rb)) return;
+        if (!grid_barrier(
+                d.sync, bl, [&](unsigned rbs) { return bookkeeping(d, bl, rbs, sim0); }, rb,
+                [&](int code) {
+                    if (lone) lone_book_writes(d, bl, code);
+                }))
+            return;
         if (threadIdx.x == 0 && lone && (f0 & F_ACTIVE) && !(f0 & (F_FROZEN | F_HOLD))) bl.clock += 1;
     }
 }
