@@ -1534,7 +1534,9 @@ __device__ __forceinline__ const T* stage_basis(const DevPtrs<T>& d) {
 }
 
 // Persistent cooperative step kernel: `nsteps` whole time steps per launch.
-// Each block takes a contiguous range of warp groups (balanced bodies per SM).
+// Each block takes a contiguous range of warp groups (balanced bodies per SM);
+// within the block the warps take them statically, or (FP32, one simulation)
+// each warp its first and then the block's next untaken one.
 template <class T, int L, int S, bool ONE, bool SPLIT, int BLK, int MINB>
 __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, int par0) {
     constexpr int WPB = BLK / 32;
