@@ -377,7 +377,8 @@ def serving_leg(fcc, oracle, work=1.5e10, pool_bodies=1 << 18, policy="fifo"):
             "pool": {"hbm_budget_bytes": budget, "max_bodies": u["max_bodies"], "max_sims": u["max_sims"]},
             "policy": policy, "served": served, "plain": plain,
             "served_over_plain": served["body_steps_per_s"] / plain["body_steps_per_s"],
-            "chunks": srv.chunks, "bitwise_equal_to_alone": f"{equal}/{len(reqs)}",
+            "chunks": srv.chunks, "device_busy_fraction": srv.device_ms * 1e-3 / max(served["makespan_s"], 1e-9),
+            "bitwise_equal_to_alone": f"{equal}/{len(reqs)}",
             "audit_force_error_vs_fp64": errs}
 
 

@@ -83,6 +83,47 @@ struct DBuf {
 // the phase loops over the rest
 inline int neighbor_grid(int64_t n) { return (int)std::min<int64_t>((n + 31) / 32, 148 * 64); }
 
+// Device staging area for host data on its way to a kernel, reused across
+// calls: it grows and never shrinks, so an admission allocates nothing once a
+// simulation of that size has been seen (allocation and release of device
+// memory synchronise the device and cost milliseconds).
+template <class V>
+struct Stage {
+    DBuf<V> buf;
+    fcc_status upload(const std::vector<V>& h, cudaStream_t st) {
+        if (h.size() > buf.n) FCC_TRY(buf.alloc(h.size(), st));
+        if (!h.empty()) CUDA_TRY(cudaMemcpyAsync(buf.p, h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice, st));
+        return FCC_OK;
+    }
+    V* p() const { return buf.p; }
+};
+
+// Device output of k_observables and its pinned host copy, grown on demand
+// and reused: an observable query allocates nothing after the first at its
+// size (allocation and release of device memory synchronise the device and
+// cost milliseconds).
+struct ObsArea {
+    DBuf<double> dev;
+    double* host = nullptr;
+    size_t cap = 0;
+    ObsArea() = default;
+    ObsArea(const ObsArea&) = delete;
+    ObsArea& operator=(const ObsArea&) = delete;
+    ~ObsArea() {
+        if (host) cudaFreeHost(host);
+    }
+    fcc_status reserve(size_t n, cudaStream_t st) {
+        if (n <= cap) return FCC_OK;
+        if (host) cudaFreeHost(host);
+        host = nullptr;
+        cap = 0;
+        FCC_TRY(dev.alloc(n, st));
+        CUDA_TRY(cudaMallocHost(&host, n * sizeof(double)));
+        cap = n;
+        return FCC_OK;
+    }
+};
+
 const double PI = 3.14159265358979323846;
 
 // Launch configurations of the step kernel: lanes per body L, node slots per
@@ -434,6 +475,7 @@ struct Engine final : EngineBase {
         ch_count, bd_idx, bd_count, flags, maxcount;
     DBuf<long long> clock, builds;
     DBuf<GridSync> sync;
+    ObsArea obs;  // perimeters / areas / shape indices: reused device and pinned host buffers
     int ccap = 1, bcap = 1;
     // pinned read-back of the run state
     struct Status {
@@ -1103,14 +1145,14 @@ struct Engine final : EngineBase {
     }
 
     fcc_status observable(int which, int32_t typ, double* out, int64_t* count) override {
-        std::vector<double> v(3 * (size_t)N);
+        const double* v = nullptr;
         if (N > 0) {
-            DBuf<double> buf;
-            FCC_TRY(buf.alloc(3 * (size_t)N, stream));
-            k_observables<T><<<(int)((N + 127) / 128), 128, 0, stream>>>(ptrs(), par(), 0, (int)N, buf.p);
+            FCC_TRY(obs.reserve(3 * (size_t)N, stream));
+            k_observables<T><<<(int)((N + 127) / 128), 128, 0, stream>>>(ptrs(), par(), 0, (int)N, obs.dev.p);
             CUDA_TRY(cudaGetLastError());
-            CUDA_TRY(cudaMemcpyAsync(v.data(), buf.p, v.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            CUDA_TRY(cudaMemcpyAsync(obs.host, obs.dev.p, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, stream));
             FCC_TRY(sync_stream());
+            v = obs.host;
         }
         int64_t w = 0;
         for (int64_t i = 0; i < N; ++i) {

@@ -230,6 +230,11 @@ struct Pool final : PoolBase {
     DBuf<GridSync> sync;
     DBuf<T> gx, gy, gth, E, glab, cs, basis;
     DBuf<MoveRange> moves;
+    std::vector<SimDesc<T>> desc_stage;  // host staging of the descriptors a compaction rebases
+    // device staging of an admission (bodies, child and bond lists), reused
+    Stage<T> st_x, st_y, st_th, st_c;
+    Stage<int> st_w, st_chc, st_chi, st_bdc, st_bdi;
+    ObsArea obs;  // perimeters / areas / shape indices: reused device and pinned host buffers
 
     struct Slot {
         bool used = false;
@@ -451,16 +456,16 @@ struct Pool final : PoolBase {
             else CUDA_TRY(cudaMemsetAsync(a.imgy.p + S.off, 0, n * sizeof(int), stream));
         }
         {
-            DBuf<int> chc, chi, bdc, bdi;
-            FCC_TRY(chc.upload(P.chc, stream));
-            FCC_TRY(chi.upload(P.chi, stream));
-            FCC_TRY(bdc.upload(P.bdc, stream));
-            FCC_TRY(bdi.upload(P.bdi, stream));
+            FCC_TRY(st_chc.upload(P.chc, stream));
+            FCC_TRY(st_chi.upload(P.chi, stream));
+            FCC_TRY(st_bdc.upload(P.bdc, stream));
+            FCC_TRY(st_bdi.upload(P.bdi, stream));
             const int64_t cnt = std::max<int64_t>(npad, nce);
             if (cnt > 0)
                 k_pool_slot_ids<<<(int)((cnt + 255) / 256), 256, 0, stream>>>(
-                    a.sim_of.p, a.cell_sim.p, a.ch_count.p, a.ch_idx.p, a.bd_count.p, a.bd_idx.p, chc.p, chi.p, bdc.p,
-                    bdi.p, s, (int)S.off, (int)N, (int)npad, S.coff, (int)nce, P.ccap, a.ccap, P.bcap, a.bcap);
+                    a.sim_of.p, a.cell_sim.p, a.ch_count.p, a.ch_idx.p, a.bd_count.p, a.bd_idx.p, st_chc.p(),
+                    st_chi.p(), st_bdc.p(), st_bdi.p(), s, (int)S.off, (int)N, (int)npad, S.coff, (int)nce, P.ccap,
+                    a.ccap, P.bcap, a.bcap);
             CUDA_TRY(cudaGetLastError());
             FCC_TRY(sync_stream());
         }
@@ -501,18 +506,16 @@ struct Pool final : PoolBase {
             }
             w[i] = (((int)S.off + P.parent[i] - 1) << 3) | (P.type[i] - 1);
         }
-        DBuf<T> bx, by, bth, bc;
-        DBuf<int> bw;
-        FCC_TRY(bx.upload(hx, stream));
-        FCC_TRY(by.upload(hy, stream));
-        FCC_TRY(bth.upload(hth, stream));
-        FCC_TRY(bc.upload(hc, stream));
-        FCC_TRY(bw.upload(w, stream));
+        FCC_TRY(st_x.upload(hx, stream));
+        FCC_TRY(st_y.upload(hy, stream));
+        FCC_TRY(st_th.upload(hth, stream));
+        FCC_TRY(st_c.upload(hc, stream));
+        FCC_TRY(st_w.upload(w, stream));
         const DevPtrs<T> d = ptrs();
         const int blocks = (int)((n + 255) / 256);
-        k_init<T><<<blocks, 256, 0, stream>>>(d, par(), (int)S.off, (int)n, bx.p, by.p, bth.p, bc.p);
+        k_init<T><<<blocks, 256, 0, stream>>>(d, par(), (int)S.off, (int)n, st_x.p(), st_y.p(), st_th.p(), st_c.p());
         CUDA_TRY(cudaGetLastError());
-        k_set_w<T><<<blocks, 256, 0, stream>>>(d, par(), (int)S.off, (int)n, bw.p);
+        k_set_w<T><<<blocks, 256, 0, stream>>>(d, par(), (int)S.off, (int)n, st_w.p());
         CUDA_TRY(cudaGetLastError());
         return sync_stream();
     }
@@ -556,6 +559,7 @@ struct Pool final : PoolBase {
         std::swap(A, B);
         cap = newcap;
         size_t k = 0;
+        int lo = nslots, hi = -1;  // the rebased descriptors go up in one copy
         for (int s : order) {
             Slot& S = slots[s];
             S.off = mv[k].new_off;
@@ -563,7 +567,16 @@ struct Pool final : PoolBase {
             ++k;
             S.spec.desc.body_off = (int)S.off;
             S.spec.desc.cell_off = S.coff;
-            CUDA_TRY(cudaMemcpyAsync(sims.p + s, &S.spec.desc, sizeof(SimDesc<T>), cudaMemcpyHostToDevice, stream));
+            lo = std::min(lo, s);
+            hi = std::max(hi, s);
+        }
+        if (hi >= lo) {
+            desc_stage.resize((size_t)(hi - lo + 1));
+            for (int s = lo; s <= hi; ++s)
+                if (slots[s].used) desc_stage[(size_t)(s - lo)] = slots[s].spec.desc;
+            // slots between lo and hi that are not in use get a copy they never read
+            CUDA_TRY(cudaMemcpyAsync(sims.p + lo, desc_stage.data(), desc_stage.size() * sizeof(SimDesc<T>),
+                                     cudaMemcpyHostToDevice, stream));
         }
         Ntot = nb;
         Ctot = nc;
@@ -1020,14 +1033,14 @@ struct Pool final : PoolBase {
         FCC_TRY(compact());
         const Slot& S = slots[s];
         const int64_t N = S.spec.N;
-        std::vector<double> v(3 * (size_t)N);
+        const double* v = nullptr;
         if (N > 0) {
-            DBuf<double> buf;
-            FCC_TRY(buf.alloc(3 * (size_t)N, stream));
-            k_observables<T><<<(int)((N + 127) / 128), 128, 0, stream>>>(ptrs(), par(), (int)S.off, (int)N, buf.p);
+            FCC_TRY(obs.reserve(3 * (size_t)N, stream));
+            k_observables<T><<<(int)((N + 127) / 128), 128, 0, stream>>>(ptrs(), par(), (int)S.off, (int)N, obs.dev.p);
             CUDA_TRY(cudaGetLastError());
-            CUDA_TRY(cudaMemcpyAsync(v.data(), buf.p, v.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            CUDA_TRY(cudaMemcpyAsync(obs.host, obs.dev.p, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, stream));
             FCC_TRY(sync_stream());
+            v = obs.host;
         }
         int64_t w = 0;
         for (int64_t i = 0; i < N; ++i) {

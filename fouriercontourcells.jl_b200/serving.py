@@ -79,6 +79,7 @@ class Server:
         self.clock = clock
         self.sleep = sleep
         self.chunks = 0
+        self.device_ms = 0.0  # device time of the pool's runs (pools that report it)
 
     def _fits_empty(self, r: Request) -> bool:
         u = self.pool.usage()
@@ -124,6 +125,9 @@ class Server:
             left = min(r.horizon - self.pool.slot(s)[1] for s, (r, _) in active.items())
             self.pool.run(max(min(self.chunk, left), min(self.min_chunk, self.chunk)))
             self.chunks += 1
+            timing = getattr(self.pool, "last_timing", None)
+            if timing is not None:
+                self.device_ms += timing()[0]
             for s in [s for s in active if self.pool.done(s)]:
                 r, adm = active.pop(s)
                 b = self.pool.bodies(s)
