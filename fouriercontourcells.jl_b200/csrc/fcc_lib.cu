@@ -156,7 +156,8 @@ const Variant VARIANTS[] = {
     {16, 3, 256, 2, step_fn<float, 16, 3, 256, 2>, nullptr, stage_bytes_per_warp<float, 16>(), 0, 2},
     {8, 5, 128, 5, step_fn<float, 8, 5, 128, 5>, nullptr, stage_bytes_per_warp<float, 8>(), 0, 3},
     {16, 3, 128, 5, step_fn<float, 16, 3, 128, 5>, nullptr, stage_bytes_per_warp<float, 16>(), 0, 2},
-    {8, 5, 224, 2, step_fn<float, 8, 5, 224, 2>, nullptr, stage_bytes_per_warp<float, 8>(), 0, 0},
+    {8, 5, 224, 2, step_fn<float, 8, 5, 224, 2>, step_fn<double, 8, 5, 224, 1>, stage_bytes_per_warp<float, 8>(),
+     stage_bytes_per_warp<double, 8>(), 0},
 };
 constexpr int NVARIANTS = sizeof(VARIANTS) / sizeof(VARIANTS[0]);
 constexpr int LANES = 8, SLOTS = 5;  // compute_gradients and the FP64 step
@@ -656,14 +657,19 @@ struct Engine final : EngineBase {
     bool one_chunk() const { return nth <= var().L * var().S; }
 
     // Variant choice.  FCC_VARIANT overrides (FP64: only variants with an FP64
-    // build).  Otherwise an FP32 one-chunk step without parent drag compares
-    // the launch shapes of the default family (bit-identical results) by the
-    // rounds of warp groups a step takes at this N, weighted by the measured
-    // time of one round: 224-thread blocks (14 warps per SM) run a round in
-    // about 0.97 of the time of 256-thread blocks but hold 12.5% fewer warps,
-    // so they win where the 256-thread grid leaves its last round part-empty
-    // (N = 1024: 10.5 vs 11.1 µs, N = 16384: 25.1 vs 25.6 µs per step) and
-    // lose where both grids fill it (N = 65536: 91.3 vs 83.1 µs).
+    // build).  Otherwise a one-chunk step without parent drag compares the
+    // launch shapes of the default family (bit-identical results, FP32 and
+    // FP64) by the rounds of warp groups a step takes at this N, weighted by
+    // the measured time of one round.  224-thread blocks (14 warps per SM in
+    // FP32, 7 in FP64) run a round in about 0.97 (FP32) or 0.945 (FP64) of the
+    // time of 256-thread blocks but hold 12.5% fewer warps.  FP32 takes its
+    // groups dynamically, so a step costs whole rounds: 224 wins where the
+    // 256-thread grid leaves its last round part-empty (N = 1024: 10.5 vs
+    // 11.1 µs, N = 16384: 25.1 vs 25.6 µs) and loses where both fill it
+    // (N = 65536: 91.3 vs 83.1 µs).  FP64 splits them statically, so a step
+    // costs the mean rounds per warp (at least one): 224 wins only while one
+    // round holds all groups (N = 1024: 14.8 vs 15.7 µs; N = 16384: 54.3 vs
+    // 52.0 µs).
     fcc_status choose_variant() {
         variant = 0;
         if (const char* e = std::getenv("FCC_VARIANT")) {
@@ -671,12 +677,12 @@ struct Engine final : EngineBase {
             if (v >= 0 && v < NVARIANTS && (sizeof(T) == 4 || VARIANTS[v].f64)) variant = v;
             return FCC_OK;
         }
-        if (sizeof(T) != 4 || N <= 0 || !one_chunk() || split) return FCC_OK;
+        if (N <= 0 || !one_chunk() || split) return FCC_OK;
         struct Candidate {
             int v;
             double round_time;
         };
-        const Candidate cands[] = {{0, 1.0}, {5, 0.97}};
+        const Candidate cands[] = {{0, 1.0}, {5, sizeof(T) == 4 ? 0.97 : 0.945}};
         double best = 1e300;
         int pick = 0;
         for (const Candidate& c : cands) {
@@ -689,8 +695,9 @@ struct Engine final : EngineBase {
             const int64_t bpw = 32 / var().L, wpb = var().blk / 32;
             const int64_t groups = (N + bpw - 1) / bpw;
             const int64_t blocks = std::min<int64_t>((groups + wpb - 1) / wpb, (int64_t)per_sm * nsm);
-            const int64_t rounds = (groups + blocks * wpb - 1) / (blocks * wpb);
-            const double cost = (double)rounds * c.round_time;
+            const double rounds = sizeof(T) == 4 ? (double)((groups + blocks * wpb - 1) / (blocks * wpb))
+                                                 : std::max(1.0, (double)groups / (double)(blocks * wpb));
+            const double cost = rounds * c.round_time;
             if (cost < best) {
                 best = cost;
                 pick = c.v;
