@@ -363,7 +363,8 @@ struct NoAfter {
 };
 // `after(code)` runs in thread 0 of the last block right after the release
 // (writes that no block reads before the next barrier).
-template <class F, class A = NoAfter>
+// LIMIT: polls before a waiting block gives up (a self-test lowers it).
+template <long long LIMIT = SPIN_LIMIT, class F, class A = NoAfter>
 __device__ __forceinline__ bool grid_barrier(GridSync* gs, BarrierLocal& bl, F&& last, unsigned bits = 0,
                                              A&& after = A{}) {
     __shared__ int s_last, s_err;
@@ -396,7 +397,7 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, BarrierLocal& bl, F&&
         long long it = 0;
         unsigned v;
         while ((v = ld_acquire(&gs->gen)) == bl.gen) {
-            if (++it > SPIN_LIMIT) {
+            if (++it > LIMIT) {
                 atomicExch(&gs->error, 1);
                 s_err = 1;
                 break;

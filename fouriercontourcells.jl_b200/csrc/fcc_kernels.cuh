@@ -1609,6 +1609,17 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
     }
 }
 
+// Self-test of the bounded barrier wait: the last block leaves without
+// arriving, so the others wait for a release that never comes; after
+// SELFTEST_POLLS polls each records gs->error and returns.  Nothing else runs.
+constexpr long long SELFTEST_POLLS = 1ll << 14;
+__global__ void k_barrier_selftest(GridSync* gs) {
+    __shared__ BarrierLocal bl;
+    barrier_start(gs, bl, false, nullptr, nullptr);
+    if (blockIdx.x == gridDim.x - 1) return;
+    grid_barrier<SELFTEST_POLLS>(gs, bl, [](unsigned) { return -1; });
+}
+
 // compute_gradients! (src/simulation.jl:150-158): forces and every gradient
 // buffer of the current state, no update.
 template <class T, int L, int S, bool ONE>

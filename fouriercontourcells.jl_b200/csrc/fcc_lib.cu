@@ -446,6 +446,7 @@ struct EngineBase {
     virtual fcc_status observable(int which, int32_t type, double* out, int64_t* count) = 0;
     virtual fcc_status body_energy(double* out) = 0;
     virtual fcc_status timing(double* ms, int64_t* launches, int64_t* steps) = 0;
+    virtual fcc_status health(int32_t* nonfinite, int32_t* barrier_error) = 0;
 };
 
 template <class T>
@@ -1171,6 +1172,17 @@ struct Engine final : EngineBase {
         return FCC_OK;
     }
 
+    fcc_status health(int32_t* nonfinite, int32_t* barrier_error) override {
+        int f = 0;
+        GridSync g{};
+        CUDA_TRY(cudaMemcpyAsync(&f, flags.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaMemcpyAsync(&g, sync.p, sizeof(GridSync), cudaMemcpyDeviceToHost, stream));
+        FCC_TRY(sync_stream());
+        if (nonfinite) *nonfinite = (f & F_NONFINITE) ? 1 : 0;
+        if (barrier_error) *barrier_error = g.error ? 1 : 0;
+        return FCC_OK;
+    }
+
     fcc_status body_energy(double* out) override {
         std::vector<T> e;
         FCC_TRY(fetch(E.p, (size_t)N, e));
@@ -1381,6 +1393,38 @@ fcc_status fcc_shape_index(fcc_sim* sim, int32_t type, double* out, int64_t* cou
 fcc_status fcc_body_energy(fcc_sim* sim, double* out) { SIM_CALL(body_energy(out)); }
 fcc_status fcc_last_timing(fcc_sim* sim, double* ms, int64_t* launches, int64_t* steps) {
     SIM_CALL(timing(ms, launches, steps));
+}
+fcc_status fcc_health(fcc_sim* sim, int32_t* nonfinite, int32_t* barrier_error) {
+    SIM_CALL(health(nonfinite, barrier_error));
+}
+
+fcc_status fcc_barrier_selftest(int32_t blocks, int32_t* error, double* ms) {
+    if (blocks < 1 || blocks > 148) return fail(FCC_ERR_ARGUMENT, "blocks must be 1..148");
+    if (!error) return fail(FCC_ERR_ARGUMENT, "null argument");
+    GridSync* gs = nullptr;
+    CUDA_TRY(cudaMalloc(&gs, sizeof(GridSync)));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaMemset(gs, 0, sizeof(GridSync));
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, 0);
+    if (e == cudaSuccess) {
+        void* args[] = {&gs};
+        e = cudaLaunchCooperativeKernel((void*)k_barrier_selftest, dim3(blocks), dim3(64), args, 0, 0);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(e1, 0);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    GridSync g{};
+    if (e == cudaSuccess) e = cudaMemcpy(&g, gs, sizeof(GridSync), cudaMemcpyDeviceToHost);
+    float t = 0.f;
+    if (e == cudaSuccess && ms) e = cudaEventElapsedTime(&t, e0, e1);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(gs);
+    CUDA_TRY(e);
+    *error = g.error ? 1 : 0;
+    if (ms) *ms = t;
+    return FCC_OK;
 }
 
 fcc_status fcc_philox_noise(uint64_t seed, uint64_t draw, int64_t nbodies, int32_t precision, double* out) {

@@ -7,6 +7,7 @@
 
 from __future__ import annotations
 
+import ctypes as C
 import math
 
 import numpy as np
@@ -24,6 +25,16 @@ def philox_noise(seed: int, draw: int, n: int, T=np.float64, lib=None, prefix="f
                                               abi.precision_bits(T), abi.dptr(out))
     abi.check(st, lib._lasterr)
     return out.T
+
+
+def barrier_selftest(blocks: int = 4, lib=None):
+    """Run the self-test of the bounded grid-barrier wait: ``blocks`` blocks
+    of which one never arrives.  Returns (error, ms): error is True when the
+    others' wait ended with the error status (expected for blocks >= 2)."""
+    lib = lib or native_library()
+    err, ms = C.c_int32(), C.c_double()
+    abi.check(lib.fcc_barrier_selftest(int(blocks), C.byref(err), C.byref(ms)), lib._lasterr)
+    return bool(err.value), ms.value
 
 
 def grid_dims(Lx, Ly, cutoff):

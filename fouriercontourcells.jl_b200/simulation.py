@@ -46,6 +46,10 @@ def native_library():
         lib.fcc_last_timing.restype = C.c_int32
         lib.fcc_version.argtypes = []
         lib.fcc_version.restype = C.c_char_p
+        lib.fcc_health.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        lib.fcc_health.restype = C.c_int32
+        lib.fcc_barrier_selftest.argtypes = [C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+        lib.fcc_barrier_selftest.restype = C.c_int32
         _LIB = lib
     return _LIB
 
@@ -251,6 +255,15 @@ class Simulation(NativeSimulation):
         ms, launches, steps = C.c_double(), C.c_int64(), C.c_int64()
         self._call("last_timing", self._h, C.byref(ms), C.byref(launches), C.byref(steps))
         return ms.value, launches.value, steps.value
+
+    def health(self):
+        """{"nonfinite", "barrier_error"}: a step produced a non-finite
+        position, angle or contour extent (until the next set_state), or a
+        grid-barrier wait of the step kernel ran out (no counterpart in the
+        reference, which checks neither)."""
+        nf, be = C.c_int32(), C.c_int32()
+        self._call("health", self._h, C.byref(nf), C.byref(be))
+        return {"nonfinite": bool(nf.value), "barrier_error": bool(be.value)}
 
 
 # ------------------------------------------------------------- functions

@@ -244,6 +244,22 @@ fcc_status fcc_build_neighbors_noalloc(int32_t precision, int64_t n, const void*
  * steps executed. */
 fcc_status fcc_last_timing(fcc_sim* sim, double* ms, int64_t* launches, int64_t* steps);
 
+/* Health of a simulation (no counterpart in the reference, which neither
+ * detects non-finite states nor waits on the device): *nonfinite = 1 once a
+ * step produced a non-finite position, angle or contour extent (sticky until
+ * fcc_set_state); *barrier_error = 1 if a grid-barrier wait of the persistent
+ * step kernel ran out of polls (the step call then failed with
+ * FCC_ERR_DEVICE). */
+fcc_status fcc_health(fcc_sim* sim, int32_t* nonfinite, int32_t* barrier_error);
+
+/* Self-test of the bounded grid-barrier wait (no counterpart in the
+ * reference): launches `blocks` blocks of which the last never arrives, so
+ * the others' wait runs out after a fixed number of polls; *error = 1 when the
+ * wait ended with the error status (the expected result for blocks >= 2; 0 for
+ * one block, which waits for no one), *ms the kernel's duration.  The device
+ * stays usable afterwards. */
+fcc_status fcc_barrier_selftest(int32_t blocks, int32_t* error, double* ms);
+
 /* ------------------------------------------------------------------ pool --
  * Many simulations packed into one engine: their bodies, grid cells and
  * neighbour lists share one device arena, and one persistent step kernel
