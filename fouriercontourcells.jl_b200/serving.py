@@ -10,10 +10,14 @@ step kernel, chunk by chunk; a simulation that reaches its horizon is read
 back (state and shape index) and retired at the end of that chunk, which
 frees its room for the requests still waiting.  Each result equals the one of
 the same request run alone with the same kernel variant, bit for bit.
+A request can be cancelled (``Server.cancel``, from the result callback or
+another thread): at the next chunk boundary it leaves the queue, or the pool
+with its state so far, and is reported with ``cancelled = True``.
 """
 
 from __future__ import annotations
 
+import threading
 import time
 from collections import deque
 from dataclasses import dataclass, field
@@ -49,6 +53,8 @@ class Result:
     finished: float
     bodies: Bodies = field(repr=False)
     shape_index_mean: float = float("nan")
+    cancelled: bool = False  # left before its horizon (bodies: the state it reached, or None if never admitted)
+    steps: int = -1          # steps taken (the horizon unless cancelled)
 
     @property
     def latency(self) -> float:
@@ -80,6 +86,19 @@ class Server:
         self.sleep = sleep
         self.chunks = 0
         self.device_ms = 0.0  # device time of the pool's runs (pools that report it)
+        self._cancel = set()
+        self._cancel_lock = threading.Lock()
+
+    def cancel(self, request_id: int):
+        """Withdraw a request: at the next chunk boundary it leaves the queue
+        or the pool (safe to call from the result callback or another thread)."""
+        with self._cancel_lock:
+            self._cancel.add(request_id)
+
+    def _take_cancelled(self):
+        with self._cancel_lock:
+            ids, self._cancel = self._cancel, set()
+        return ids
 
     def _fits_empty(self, r: Request) -> bool:
         u = self.pool.usage()
@@ -98,6 +117,20 @@ class Server:
         t0 = self.clock()
         now = lambda: self.clock() - t0
         while pending or waiting or active:
+            ids = self._take_cancelled()
+            if ids:
+                for q in [q for q in list(waiting) + list(pending) if q.id in ids]:  # never admitted
+                    results.append(Result(q.id, q.bodies.n, q.horizon, q.arrival, float("nan"), now(), None,
+                                          cancelled=True, steps=0))
+                waiting = deque(q for q in waiting if q.id not in ids)
+                pending = deque(q for q in pending if q.id not in ids)
+                for s in [s for s, (r, _) in active.items() if r.id in ids]:
+                    r, adm = active.pop(s)
+                    steps = self.pool.slot(s)[1]
+                    b = self.pool.bodies(s)
+                    self.pool.remove(s)
+                    results.append(Result(r.id, r.bodies.n, r.horizon, r.arrival, adm, now(), b, cancelled=True,
+                                          steps=steps))
             t = now()
             while pending and pending[0].arrival <= t:
                 waiting.append(pending.popleft())
@@ -134,7 +167,7 @@ class Server:
                 si = self.pool.shape_index(s)
                 self.pool.remove(s)
                 res = Result(r.id, r.bodies.n, r.horizon, r.arrival, adm, now(), b,
-                             float(np.mean(si)) if len(si) else float("nan"))
+                             float(np.mean(si)) if len(si) else float("nan"), steps=r.horizon)
                 results.append(res)
                 if on_result:
                     on_result(res)
@@ -142,13 +175,15 @@ class Server:
 
 
 def summary(results, makespan=None):
-    """p50/p99 time to result and body-steps/s of a served stream."""
-    lat = np.array([r.latency for r in results])
-    work = sum(r.n * r.horizon for r in results)
+    """p50/p99 time to result and body-steps/s of a served stream (completed
+    requests; cancelled ones are counted apart, with the steps they took)."""
+    done = [r for r in results if not r.cancelled]
+    lat = np.array([r.latency for r in done]) if done else np.array([float("nan")])
+    work = sum(r.n * r.horizon for r in done) + sum(r.n * max(r.steps, 0) for r in results if r.cancelled)
     span = makespan if makespan is not None else max(r.finished for r in results) - min(r.arrival for r in results)
-    return {"requests": len(results), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-            "mean_s": float(lat.mean()), "body_steps": int(work), "makespan_s": float(span),
-            "body_steps_per_s": work / span if span > 0 else float("nan")}
+    return {"requests": len(done), "cancelled": len(results) - len(done), "p50_s": float(np.percentile(lat, 50)),
+            "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()), "body_steps": int(work),
+            "makespan_s": float(span), "body_steps_per_s": work / span if span > 0 else float("nan")}
 
 
 def sequential_latencies(arrivals, durations):

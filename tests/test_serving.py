@@ -141,3 +141,31 @@ def test_sjf_admits_small_work_first_and_backfills():
     assert [r.id for r in res][-1] == 0
     with pytest.raises(fcc.ArgumentError):
         fcc.Server(pool, policy="lifo")
+
+
+def test_cancelled_requests_leave_the_queue_and_the_pool():
+    """A request cancelled while it runs leaves the pool with the state it
+    reached; one cancelled while it waits never runs; the others are
+    unaffected (SURVEY: a cancelled request as a host-injected fault)."""
+    clk = FakeClock()
+    pool = FakePool(clk, max_bodies=160, max_sims=4)
+    # r0 long and running, r1 short and running, r2 waits for room
+    reqs = [req(0, 8, 12, 5000, 0.0), req(1, 8, 6, 300, 0.0), req(2, 8, 12, 400, 0.01), req(3, 2, 4, 200, 0.02)]
+    srv = fcc.Server(pool, chunk=256, min_chunk=1, clock=clk, sleep=clk.sleep)
+
+    def on_result(res):
+        if res.id == 1:  # when r1 finishes: cancel r0 (running) and r2 (still waiting)
+            srv.cancel(0)
+            srv.cancel(2)
+
+    res = {r.id: r for r in srv.serve(reqs, on_result=on_result)}
+    assert set(res) == {0, 1, 2, 3}
+    assert res[0].cancelled and 0 < res[0].steps < 5000 and res[0].bodies is not None
+    assert res[2].cancelled and res[2].steps == 0 and res[2].bodies is None
+    assert not res[1].cancelled and res[1].steps == 300
+    assert not res[3].cancelled and res[3].steps == 200
+    assert not any(e[0] == "add" and e[1] == 2 for e in pool.log)  # r2 never entered the pool
+    assert ("remove", 0) in [(e[0], e[1]) for e in pool.log]
+    assert pool.usage()["sims"] == 0
+    s = serving.summary(list(res.values()))
+    assert s["requests"] == 2 and s["cancelled"] == 2
