@@ -50,3 +50,25 @@ def test_barrier_wait_runs_out_with_an_error_status():
     s.run(20)
     assert np.isfinite(s.bodies.x).all()
     assert s.health() == {"nonfinite": False, "barrier_error": False}
+
+
+def test_state_outside_the_box_matches_the_oracle():
+    """Positions written from the host outside [0, L) (a host-injected fault:
+    the reference would index its cell grid out of bounds) are clamped into
+    the grid for the cell list and wrapped by the first update, with image
+    counters; FP64 against the oracle after 30 steps (rtol 1e-8)."""
+    from conftest import oracle
+    b, box, kw = small(9)
+    bad = b.copy()
+    bad.x[:5] += box.Lx
+    bad.y[5:10] -= 2 * box.Ly
+    g = fcc.Simulation(bad, box, T=np.float64, **kw)
+    g.run(30)
+    o = oracle.OracleSimulation(bad, box, T=np.float64, **kw)
+    o.step(30)
+    a, c = g.bodies, o.bodies
+    assert np.allclose(a.x, c.x, rtol=1e-8) and np.allclose(a.y, c.y, rtol=1e-8)
+    assert np.allclose(a.coef, c.coef, rtol=1e-8, atol=1e-12)
+    assert np.array_equal(a.imgx, c.imgx) and np.array_equal(a.imgy, c.imgy)
+    assert (a.x >= 0).all() and (a.x < box.Lx).all() and (a.y >= 0).all() and (a.y < box.Ly).all()
+    assert g.health() == {"nonfinite": False, "barrier_error": False}
