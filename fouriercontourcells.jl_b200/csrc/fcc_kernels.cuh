@@ -690,6 +690,24 @@ __device__ __forceinline__ void load_update_pre(const DevPtrs<T>& d, int gg, int
 
 // (cos n t, sin n t) from (cos t, sin t) by binary powering, n = 2..10 (a
 // few complex products instead of one sincos per mode).
+// Per-mode pieces of the end of a step, shared by the update and by k_init so
+// that a state loaded with set_state continues exactly as the run that wrote
+// it: |(a, b)| for rmax and the projection, its FP64 square for a0, and the
+// rotation into the lab frame.
+template <class T>
+__device__ __forceinline__ T mode_norm(T a, T b) {
+    return t_sqrt(a * a + b * b);
+}
+template <class T>
+__device__ __forceinline__ double mode_sq(T a, T b) {
+    return (double)a * (double)a + (double)b * (double)b;
+}
+template <class T>
+__device__ __forceinline__ void to_lab(T a, T b, T co, T so, T& al, T& be) {
+    al = a * co - b * so;
+    be = a * so + b * co;
+}
+
 template <class T>
 __device__ __forceinline__ void cis_pow(T c1, T s1, int n, T& cn, T& sn) {
     T rc = T(1), rs = T(0), bc = c1, bs = s1;
@@ -786,7 +804,7 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
             const T gcb = -ga * so + gb * co - h0 * b;
             an[u] = a - dtmu * gca;
             bn[u] = b - dtmu * gcb;
-            sp += (double)t_sqrt(an[u] * an[u] + bn[u] * bn[u]);
+            sp += (double)mode_norm(an[u], bn[u]);
         }
     }
     // enforce_shape! (src/dynamics.jl:44-64) with FP64 sums
@@ -801,7 +819,7 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
     }
     double qp = 0.0;
 #pragma unroll
-    for (int u = 0; u < MPL; ++u) qp += (double)an[u] * (double)an[u] + (double)bn[u] * (double)bn[u];
+    for (int u = 0; u < MPL; ++u) qp += mode_sq(an[u], bn[u]);
     const double qs = group_sum<L>(qp);
     const T a0n = T(sqrt(1.0 - qs * 0.5));
 
@@ -812,11 +830,10 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
     for (int u = 0; u < MPL; ++u) {
         const int m = l + u * L;
         if (m < K) {
-            T so, co;
+            T so, co, al, be;
             cis_pow(cn1, sn1, m + 2, co, so);
-            const T al = an[u] * co - bn[u] * so;
-            const T be = an[u] * so + bn[u] * co;
-            bp += t_sqrt(an[u] * an[u] + bn[u] * bn[u]);
+            to_lab(an[u], bn[u], co, so, al, be);
+            bp += mode_norm(an[u], bn[u]);
             if (act) {
                 rn[r_al(m)] = r0 * al;
                 rn[r_be(m)] = r0 * be;
@@ -1735,8 +1752,27 @@ __global__ void k_init(DevPtrs<T> d, int par, int g0, int n, const T* __restrict
     T c[NCM];
 #pragma unroll
     for (int r = 0; r < NCM; ++r) c[r] = coef_in[(size_t)i * NCM + r];
-    double ssum = 0.0;
-    for (int m = 0; m < K; ++m) ssum += sqrt((double)c[1 + m] * c[1 + m] + (double)c[1 + KM + m] * c[1 + KM + m]);
+    // enforce_shape! and the lab frame with the arithmetic of the update's
+    // end of step (update_body): modes spread over 8 lanes as m = lane + 8u,
+    // per-lane sums in u order, lanes combined by the xor butterfly of
+    // group_sum<8>, so a state written by a run and loaded again continues
+    // bit for bit (for the 8-lane launch shapes)
+    constexpr int LV = 8, MV = (KM + LV - 1) / LV;
+    auto tree8 = [](auto* v) {  // ((v0+v4)+(v2+v6)) + ((v1+v5)+(v3+v7)), as group_sum<8>
+        return ((v[0] + v[4]) + (v[2] + v[6])) + ((v[1] + v[5]) + (v[3] + v[7]));
+    };
+    double spl[LV];
+#pragma unroll
+    for (int l = 0; l < LV; ++l) {
+        double sp = 0.0;
+#pragma unroll
+        for (int u = 0; u < MV; ++u) {
+            const int m = l + u * LV;
+            if (m < K) sp += (double)mode_norm(c[1 + m], c[1 + KM + m]);
+        }
+        spl[l] = sp;
+    }
+    const double ssum = tree8(spl);
     if (ssum > SHAPE_BOUND) {
         const double f = SHAPE_BOUND / ssum;
         for (int m = 0; m < K; ++m) {
@@ -1744,26 +1780,45 @@ __global__ void k_init(DevPtrs<T> d, int par, int g0, int n, const T* __restrict
             c[1 + KM + m] = T((double)c[1 + KM + m] * f);
         }
     }
-    double q = 0.0;
-    for (int m = 0; m < K; ++m) q += (double)c[1 + m] * c[1 + m] + (double)c[1 + KM + m] * c[1 + KM + m];
-    c[0] = T(sqrt(1.0 - q * 0.5));
+    double qpl[LV];
+#pragma unroll
+    for (int l = 0; l < LV; ++l) {
+        double qp = 0.0;
+#pragma unroll
+        for (int u = 0; u < MV; ++u) {
+            const int m = l + u * LV;
+            qp += m < K ? mode_sq(c[1 + m], c[1 + KM + m]) : 0.0;
+        }
+        qpl[l] = qp;
+    }
+    c[0] = T(sqrt(1.0 - tree8(qpl) * 0.5));
     const T r0 = d.R0[g];
     T* rn = rec_cur_mut(d, par) + (size_t)g * RECW;
     T* ro = rec_next(d, par) + (size_t)g * RECW;
-    T bound = c[0];
     for (int r = 0; r < RECW; ++r) ro[r] = T(0);
-    for (int m = 0; m < KM; ++m) {
-        T al = T(0), be = T(0);
-        if (m < K) {
-            T so, co;
-            t_sincos(T(m + 2) * th[i], &so, &co);
-            al = c[1 + m] * co - c[1 + KM + m] * so;
-            be = c[1 + m] * so + c[1 + KM + m] * co;
-            bound += t_sqrt(c[1 + m] * c[1 + m] + c[1 + KM + m] * c[1 + KM + m]);
+    T s1, c1;
+    t_sincos(th[i], &s1, &c1);
+    T bpl[LV];
+#pragma unroll
+    for (int l = 0; l < LV; ++l) {
+        T bp = T(0);
+#pragma unroll
+        for (int u = 0; u < MV; ++u) {
+            const int m = l + u * LV;
+            if (m >= KM) continue;
+            T al = T(0), be = T(0);
+            if (m < K) {
+                T so, co;
+                cis_pow(c1, s1, m + 2, co, so);
+                to_lab(c[1 + m], c[1 + KM + m], co, so, al, be);
+                bp += mode_norm(c[1 + m], c[1 + KM + m]);
+            }
+            rn[r_al(m)] = r0 * al;
+            rn[r_be(m)] = r0 * be;
         }
-        rn[r_al(m)] = r0 * al;
-        rn[r_be(m)] = r0 * be;
+        bpl[l] = bp;
     }
+    const T bound = c[0] + tree8(bpl);
     rn[R_X] = x[i];
     rn[R_Y] = y[i];
     rn[R_RMAX] = r0 * bound;
