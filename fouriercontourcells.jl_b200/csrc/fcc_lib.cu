@@ -25,6 +25,27 @@
 #include "../../include/fcc.h"
 #include "fcc_kernels.cuh"
 
+#ifndef FCC_NVTX
+#define FCC_NVTX 1  // named ranges around the host phases for nsys / ncu timelines (free without a tool)
+#endif
+#if FCC_NVTX
+#include <nvtx3/nvToolsExt.h>
+#endif
+
+namespace fcc {
+// A named range on the profiler timeline for the lifetime of the object.
+struct Range {
+#if FCC_NVTX
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+#else
+    explicit Range(const char*) {}
+#endif
+    Range(const Range&) = delete;
+    Range& operator=(const Range&) = delete;
+};
+}  // namespace fcc
+
 using namespace fcc;
 
 namespace {
@@ -854,6 +875,7 @@ struct Engine final : EngineBase {
     // freezes the simulation on the device (the remaining launched steps do
     // nothing); the host then regrows the list and launches the missing steps.
     fcc_status advance(int64_t n, int per) {
+        Range range("fcc advance");
         int64_t done = 0;
         while (done < n) {
             const long long start = clock_h;
@@ -910,6 +932,7 @@ struct Engine final : EngineBase {
     }
 
     fcc_status update_neighbors(bool force) override {
+        Range range("fcc update_neighbors");
         if (!has_contact || N == 0) return FCC_OK;
         const DevPtrs<T> d = ptrs();
         const int grid = (int)((N + 255) / 256);
@@ -947,6 +970,7 @@ struct Engine final : EngineBase {
     }
 
     fcc_status compute_gradients() override {
+        Range range("fcc compute_gradients");
         if (N == 0) return FCC_OK;
         FCC_TRY(ensure_diag());
         const DevPtrs<T> d = ptrs();

@@ -408,6 +408,7 @@ struct Pool final : PoolBase {
 
     // ------------------------------------------------------- admission --
     fcc_status add(const fcc_params* p, const fcc_bodies_host* b, int64_t horizon, int32_t* slot_out) override {
+        Range range("fcc pool add");
         if (!p || !b || !slot_out) return fail(FCC_ERR_ARGUMENT, "null argument");
         if (p->precision != (sizeof(T) == 4 ? 32 : 64))
             return fail(FCC_ERR_ARGUMENT, "pool: the simulation's precision differs from the pool's");
@@ -536,6 +537,7 @@ struct Pool final : PoolBase {
     // Gather every live simulation into B at dense offsets (list capacity
     // newcap), swap the arena copies, rebase the descriptors.
     fcc_status gather(int newcap) {
+        Range range("fcc pool compact");
         std::vector<MoveRange> mv;
         int64_t nb = 0, nc = 0;
         for (int s : order) {
@@ -688,6 +690,7 @@ struct Pool final : PoolBase {
     }
 
     fcc_status run_round(int64_t most) {
+        Range range("fcc pool round");
         FCC_TRY(configure());
         const int64_t nl = (most + spl - 1) / spl;
         if (use_graph && graph_ok) {
@@ -874,6 +877,7 @@ struct Pool final : PoolBase {
     }
 
     fcc_status tune(int64_t steps, bool reorder, int32_t* chosen, double* best_us) override {
+        Range range("fcc pool tune");
         FCC_TRY(compact());
         if (order.empty()) return fail(FCC_ERR_ARGUMENT, "pool: nothing to tune on (no simulations)");
         if (steps < 1) return fail(FCC_ERR_ARGUMENT, "pool: tune needs at least one step");
