@@ -189,7 +189,8 @@ __global__ void k_pool_slot_ids(int* sim_of, int* cell_sim, int* ch_count, int* 
 
 struct PoolBase {
     virtual ~PoolBase() = default;
-    virtual fcc_status add(const fcc_params* p, const fcc_bodies_host* b, int64_t horizon, int32_t* slot) = 0;
+    virtual fcc_status add(const fcc_params* p, const fcc_bodies_host* b, int64_t horizon, int64_t clock0,
+                           int32_t* slot) = 0;
     virtual fcc_status remove(int32_t slot) = 0;
     virtual fcc_status run(int64_t n) = 0;
     virtual fcc_status slot_info(int32_t slot, int32_t* active, int64_t* steps, int64_t* horizon) = 0;
@@ -407,9 +408,11 @@ struct Pool final : PoolBase {
     }
 
     // ------------------------------------------------------- admission --
-    fcc_status add(const fcc_params* p, const fcc_bodies_host* b, int64_t horizon, int32_t* slot_out) override {
+    fcc_status add(const fcc_params* p, const fcc_bodies_host* b, int64_t horizon, int64_t clock0,
+                   int32_t* slot_out) override {
         Range range("fcc pool add");
         if (!p || !b || !slot_out) return fail(FCC_ERR_ARGUMENT, "null argument");
+        if (clock0 < 0) return fail(FCC_ERR_ARGUMENT, "pool: clock must be >= 0");
         if (p->precision != (sizeof(T) == 4 ? 32 : 64))
             return fail(FCC_ERR_ARGUMENT, "pool: the simulation's precision differs from the pool's");
         if (p->ntheta != nth) return fail(FCC_ERR_DIMENSION, "pool: the simulation's ntheta differs from the pool's");
@@ -442,6 +445,11 @@ struct Pool final : PoolBase {
         S.coff = (int)Ctot;
         S.ncells = (int)nce;
         S.horizon = horizon;
+        // a resumed simulation counts its steps (and time) from its clock, so
+        // that steps done and the horizon are both measured on the clock
+        S.clock_h = clock0;
+        S.step_h = clock0;
+        S.t_h = (T)((double)clock0 * (double)sp.desc.dt);
         sp.desc.body_off = (int)S.off;
         sp.desc.cell_off = S.coff;
         S.spec = std::move(sp);
@@ -480,7 +488,7 @@ struct Pool final : PoolBase {
         S.flags_h = F_ACTIVE | F_HOLD | (P.has_contact ? F_CONTACT : 0);
         const long long zero = 0;
         CUDA_TRY(cudaMemcpyAsync(flags.p + s, &S.flags_h, sizeof(int), cudaMemcpyHostToDevice, stream));
-        CUDA_TRY(cudaMemcpyAsync(clock.p + s, &zero, sizeof(long long), cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(cudaMemcpyAsync(clock.p + s, &S.clock_h, sizeof(long long), cudaMemcpyHostToDevice, stream));
         CUDA_TRY(cudaMemcpyAsync(builds.p + s, &zero, sizeof(long long), cudaMemcpyHostToDevice, stream));
         CUDA_TRY(cudaMemsetAsync(maxcount.p + s, 0, sizeof(int), stream));
         *slot_out = s;
@@ -1151,7 +1159,11 @@ fcc_status fcc_pool_destroy(fcc_pool* pool) {
 
 fcc_status fcc_pool_add(fcc_pool* pool, const fcc_params* params, const fcc_bodies_host* bodies, int64_t horizon,
                         int32_t* slot) {
-    POOL_CALL(add(params, bodies, horizon, slot));
+    POOL_CALL(add(params, bodies, horizon, 0, slot));
+}
+fcc_status fcc_pool_add_at(fcc_pool* pool, const fcc_params* params, const fcc_bodies_host* bodies, int64_t clock,
+                           int64_t horizon, int32_t* slot) {
+    POOL_CALL(add(params, bodies, horizon, clock, slot));
 }
 fcc_status fcc_pool_remove(fcc_pool* pool, int32_t slot) { POOL_CALL(remove(slot)); }
 fcc_status fcc_pool_run(fcc_pool* pool, int64_t n) { POOL_CALL(run(n)); }

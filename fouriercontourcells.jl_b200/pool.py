@@ -27,6 +27,8 @@ _POOL_SIG = {
     "pool_destroy": [C.c_void_p],
     "pool_add": [C.c_void_p, C.POINTER(abi.FccParams), C.POINTER(abi.FccBodiesHost), C.c_int64,
                  C.POINTER(C.c_int32)],
+    "pool_add_at": [C.c_void_p, C.POINTER(abi.FccParams), C.POINTER(abi.FccBodiesHost), C.c_int64, C.c_int64,
+                    C.POINTER(C.c_int32)],
     "pool_remove": [C.c_void_p, C.c_int32],
     "pool_run": [C.c_void_p, C.c_int64],
     "pool_slot": [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
@@ -132,13 +134,18 @@ class Pool:
 
     # ------------------------------------------------------------ slots
     def add(self, bodies: Bodies, box, types, energies=(), bonds=(), dt=0.005, seed=1, skin=0.3, horizon=0,
-            nl_capacity=32) -> int:
+            nl_capacity=32, clock=0) -> int:
         """Admit a simulation (the arguments of ``Simulation``); raises PoolFull
-        when it does not fit now."""
+        when it does not fit now.  ``clock`` > 0 resumes a checkpoint (the
+        state and clock ``state`` returned): it holds at clock ``horizon``."""
         params = abi.ParamsBuffer(box, types, energies, bonds, dt, self.nθ, self.T, seed, skin, nl_capacity)
         buf = abi.BodiesBuffer.from_bodies(bodies)
         slot = C.c_int32()
-        self._call("pool_add", self._h, C.byref(params.p), C.byref(buf.s), int(horizon), C.byref(slot))
+        if clock:
+            self._call("pool_add_at", self._h, C.byref(params.p), C.byref(buf.s), int(clock), int(horizon),
+                       C.byref(slot))
+        else:
+            self._call("pool_add", self._h, C.byref(params.p), C.byref(buf.s), int(horizon), C.byref(slot))
         self._slots[slot.value] = (bodies.n, bodies.ncoef, np.array(bodies.type, dtype=np.int32), box)
         return slot.value
 

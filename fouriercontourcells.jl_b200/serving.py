@@ -24,7 +24,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .model import ArgumentError, Bodies, PeriodicBox
+from .model import ArgumentError, Bodies, DeviceError, PeriodicBox
 from .pool import grid_cells, padded
 
 
@@ -71,13 +71,20 @@ class Server:
     "fifo" admits in arrival order (a request that does not fit yet blocks the
     ones behind it); "sjf" admits the waiting requests with the least work
     (bodies × horizon) first and fills the room with any that fit (lower
-    median time to result under overload; large requests wait longer)."""
+    median time to result under overload; large requests wait longer);
+    "evict" is "sjf" that also makes room for a waiting request by evicting
+    the running one with the most work left, if that is at least
+    ``evict_ratio`` times the waiting one's: the evicted request keeps its
+    state and clock and is re-admitted later where it stopped (the pool's
+    admission at a clock), so its result is still that of its solo run."""
 
     def __init__(self, pool, chunk=512, min_chunk=32, T=np.float32, clock=time.perf_counter, sleep=time.sleep,
-                 policy="fifo"):
-        if policy not in ("fifo", "sjf"):
-            raise ArgumentError("policy must be 'fifo' or 'sjf'")
+                 policy="fifo", evict_ratio=4.0):
+        if policy not in ("fifo", "sjf", "evict"):
+            raise ArgumentError("policy must be 'fifo', 'sjf' or 'evict'")
         self.policy = policy
+        self.evict_ratio = float(evict_ratio)
+        self.evictions = 0
         self.pool = pool
         self.chunk = int(chunk)
         self.min_chunk = int(min_chunk)
@@ -112,16 +119,35 @@ class Server:
             if not self._fits_empty(r):
                 raise ArgumentError(f"request {r.id} ({r.bodies.n} bodies) does not fit in an empty pool")
         waiting = deque()
-        active = {}  # slot -> (request, admitted)
+        active = {}  # slot -> (request, first admitted)
         results = []
+        resume = {}  # request id -> (state, clock) of an evicted request
+        first = {}   # request id -> first admission time
         t0 = self.clock()
         now = lambda: self.clock() - t0
+
+        def left_of(q):  # body-steps a waiting request has left
+            return q.bodies.n * (q.horizon - (resume[q.id][1] if q.id in resume else 0))
+
+        def admit(q):
+            if q.id in resume:
+                b, c = resume[q.id]
+                slot = self.pool.try_add(b, q.box, horizon=q.horizon, clock=c, **q.kw)
+            else:
+                slot = self.pool.try_add(q.bodies, q.box, horizon=q.horizon, **q.kw)
+            if slot is not None:
+                resume.pop(q.id, None)
+                first.setdefault(q.id, now())
+                active[slot] = (q, first[q.id])
+            return slot
+
         while pending or waiting or active:
             ids = self._take_cancelled()
             if ids:
-                for q in [q for q in list(waiting) + list(pending) if q.id in ids]:  # never admitted
-                    results.append(Result(q.id, q.bodies.n, q.horizon, q.arrival, float("nan"), now(), None,
-                                          cancelled=True, steps=0))
+                for q in [q for q in list(waiting) + list(pending) if q.id in ids]:  # not running
+                    b, c = resume.pop(q.id, (None, 0))
+                    results.append(Result(q.id, q.bodies.n, q.horizon, q.arrival, first.get(q.id, float("nan")),
+                                          now(), b, cancelled=True, steps=c))
                 waiting = deque(q for q in waiting if q.id not in ids)
                 pending = deque(q for q in pending if q.id not in ids)
                 for s in [s for s, (r, _) in active.items() if r.id in ids]:
@@ -136,28 +162,39 @@ class Server:
                 waiting.append(pending.popleft())
             if self.policy == "fifo":
                 while waiting:  # admission in arrival order, as slots and memory free up
-                    r = waiting[0]
-                    slot = self.pool.try_add(r.bodies, r.box, horizon=r.horizon, **r.kw)
-                    if slot is None:
+                    if admit(waiting[0]) is None:
                         break
                     waiting.popleft()
-                    active[slot] = (r, now())
-            else:  # smallest work first; every waiting request that fits is admitted
-                admitted = set()
-                for r in sorted(waiting, key=lambda q: (q.work, q.arrival)):
-                    slot = self.pool.try_add(r.bodies, r.box, horizon=r.horizon, **r.kw)
+            else:  # least work left first; every waiting request that fits is admitted
+                admitted, evicted = set(), []
+                for r in sorted(waiting, key=lambda q: (left_of(q), q.arrival)):
+                    slot = admit(r)
+                    while slot is None and self.policy == "evict" and active:
+                        work_left = {s: v.bodies.n * (v.horizon - self.pool.slot(s)[1]) for s, (v, _) in active.items()}
+                        s = max(work_left, key=work_left.get)
+                        if work_left[s] < self.evict_ratio * left_of(r):
+                            break
+                        v, _ = active.pop(s)
+                        resume[v.id] = (self.pool.bodies(s), self.pool.slot(s)[1])
+                        self.pool.remove(s)
+                        self.evictions += 1
+                        evicted.append(v)
+                        slot = admit(r)
                     if slot is not None:
                         admitted.add(id(r))
-                        active[slot] = (r, now())
                 if admitted:
                     waiting = deque(q for q in waiting if id(q) not in admitted)
+                waiting.extend(evicted)
             if not active:
                 if pending:
                     self.sleep(max(0.0, pending[0].arrival - now()))
                 continue
-            left = min(r.horizon - self.pool.slot(s)[1] for s, (r, _) in active.items())
+            before = {s: self.pool.slot(s)[1] for s in active}
+            left = min(r.horizon - before[s] for s, (r, _) in active.items())
             self.pool.run(max(min(self.chunk, left), min(self.min_chunk, self.chunk)))
             self.chunks += 1
+            if all(self.pool.slot(s)[1] == before[s] and not self.pool.done(s) for s in active):
+                raise DeviceError("serving: a pool round advanced no simulation and none is done")
             timing = getattr(self.pool, "last_timing", None)
             if timing is not None:
                 self.device_ms += timing()[0]

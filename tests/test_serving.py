@@ -37,14 +37,14 @@ class FakePool:
         return dict(bodies=sum(serving.padded(s["n"]) for s in self.sims.values()),
                     cells=sum(s["cells"] for s in self.sims.values()), sims=len(self.sims), **self.cap)
 
-    def try_add(self, bodies, box, horizon, **kw):
+    def try_add(self, bodies, box, horizon, clock=0, **kw):
         u = self.usage()
         cells = serving.grid_cells(box, bodies.R0, kw.get("skin", 0.3), np.float32)
         if (u["sims"] >= u["max_sims"] or u["bodies"] + serving.padded(bodies.n) > u["max_bodies"]
                 or u["cells"] + cells > u["max_cells"]):
             return None
         slot = min(set(range(self.cap["max_sims"])) - set(self.sims))
-        self.sims[slot] = dict(n=bodies.n, cells=cells, horizon=horizon, steps=0, seed=kw["seed"], bodies=bodies)
+        self.sims[slot] = dict(n=bodies.n, cells=cells, horizon=horizon, steps=clock, seed=kw["seed"], bodies=bodies)
         self.log.append(("add", kw["seed"], self.clock.t))
         return slot
 
@@ -169,3 +169,38 @@ def test_cancelled_requests_leave_the_queue_and_the_pool():
     assert pool.usage()["sims"] == 0
     s = serving.summary(list(res.values()))
     assert s["requests"] == 2 and s["cancelled"] == 2
+
+
+def test_evict_policy_makes_room_and_resumes_where_it_stopped():
+    """A short request that does not fit evicts the running request with the
+    most work left; the evicted one is re-admitted at the clock it reached
+    (its state saved) and still ends at its horizon."""
+    clk = FakeClock()
+    pool = FakePool(clk, max_bodies=128, max_sims=8)
+    # r0 (96 bodies, long) runs alone; r1 (64 bodies, short) arrives and does not fit beside it
+    reqs = [req(0, 8, 12, 4000, 0.0), req(1, 8, 8, 200, 0.001)]
+    srv = fcc.Server(pool, chunk=128, min_chunk=1, clock=clk, sleep=clk.sleep, policy="evict")
+    res = {r.id: r for r in srv.serve(reqs)}
+    assert srv.evictions >= 1
+    adds = [e for e in pool.log if e[0] == "add"]
+    assert [e[1] for e in adds][:3] == [0, 1, 0]        # r0, r1 in r0's place, r0 again
+    assert res[1].finished < res[0].finished
+    assert not res[0].cancelled and res[0].steps == 4000
+    with pytest.raises(fcc.ArgumentError):
+        fcc.Server(pool, policy="lru")
+
+
+def test_a_round_without_progress_raises_instead_of_looping():
+    """A pool whose step counts stop moving short of the horizon (a slot
+    held by mistake) makes the loop raise DeviceError instead of spinning."""
+    clk = FakeClock()
+
+    class StuckPool(FakePool):
+        def run(self, n):
+            self.clock.t += 1e-3
+
+    pool = StuckPool(clk)
+    srv = fcc.Server(pool, chunk=64, min_chunk=1, clock=clk, sleep=clk.sleep)
+    with pytest.raises(fcc.DeviceError):
+        srv.serve([req(0, 4, 4, 100, 0.0)])
+    assert srv.chunks == 1
