@@ -303,9 +303,10 @@ fcc_status fcc_pool_add(fcc_pool* pool, const fcc_params* params, const fcc_bodi
                         int32_t* slot);
 /* Admit a simulation resumed from a checkpoint: `bodies` and `clock` as
  * fcc_get_state / fcc_pool_get_state returned them (the clock is the Philox
- * draw index, src/random.jl:103); it holds when its clock reaches `horizon`.
- * It continues bit for bit as the run that wrote the checkpoint (no
- * counterpart in the reference: the serving loop evicts and re-admits with it). */
+ * draw index, src/random.jl:103); it holds when its clock reaches `horizon`,
+ * and its steps done count from `clock`.  The state is loaded with the same
+ * arithmetic as fcc_set_state (no counterpart in the reference: the serving
+ * loop evicts and re-admits with it). */
 fcc_status fcc_pool_add_at(fcc_pool* pool, const fcc_params* params, const fcc_bodies_host* bodies, int64_t clock,
                            int64_t horizon, int32_t* slot);
 /* Retire a simulation; its room is reclaimed before the next run or add. */
