@@ -264,7 +264,7 @@ fcc_status make_spec(const fcc_params* p, const fcc_bodies_host* b, SimSpec<T>& 
     if (!(nth > 2 * (K + 1))) return fail(FCC_ERR_ARGUMENT, "nθ must exceed 2·maxmode");
     nc = 2 * K + 1;
     if (b->ncoef != nc) return fail(FCC_ERR_DIMENSION, "coefficient rows must be odd: [a₀; aₙ; bₙ]");
-    if (K > KM) return fail(FCC_ERR_UNSUPPORTED, "this build supports maxmode ≤ 10");
+    if (K > KM) return fail(FCC_ERR_UNSUPPORTED, "the kernels support maxmode ≤ 10");
     if (!(p->skin >= 0)) return fail(FCC_ERR_ARGUMENT, "skin must be non-negative");
 
     // simulation descriptor (convert_precision: every parameter to T)

@@ -44,7 +44,7 @@ enum {
     FCC_ERR_ARGUMENT = 1,    /* reference: ArgumentError */
     FCC_ERR_DIMENSION = 2,   /* reference: DimensionMismatch */
     FCC_ERR_CUDA = 3,        /* CUDA runtime error (message has the CUDA text) */
-    FCC_ERR_UNSUPPORTED = 4, /* valid model outside this build's kernels */
+    FCC_ERR_UNSUPPORTED = 4, /* valid model outside these kernels */
     FCC_ERR_DEVICE = 5,      /* device-side error status (e.g. non-finite state) */
     FCC_ERR_NOMEM = 6,       /* device allocation failed */
     FCC_ERR_FULL = 7         /* pool: no room for this simulation until others leave */

@@ -1,6 +1,6 @@
 // fcc_oracle.cpp — CPU oracle of the FourierContourCells.jl time step.
 //
-// TEST INFRASTRUCTURE ONLY: the parity checker of tests/ and the timed CPU
+// TEST INFRASTRUCTURE ONLY: the parity reference of tests/ and the timed CPU
 // baseline of bench.py.  The product library never links or calls it.
 //
 // A plain restatement of the reference's CPU path, function by function, in

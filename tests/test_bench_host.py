@@ -6,7 +6,7 @@ At a near-tie the Overlap pressure g = J H(d) of a contour node may sit on
 the other side of zero in FP32 (rounding of d is about 1e-5 at coordinates
 of 100), which moves that body's force by O(J).  The check excludes exactly
 those bodies (a node pressure apart by at least J/2) and counts them; every
-other body must agree with FP64 to the north-star bound of 1e-5 of each
+other body must agree with FP64 to the stated bound of 1e-5 of each
 field's scale."""
 
 import importlib.util

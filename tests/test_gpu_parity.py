@@ -264,7 +264,7 @@ def test_two_discs_overlap_force_chunked():
     assert math.isclose(gr.gx[1], -math.sqrt(4 - d * d), rel_tol=1e-3)
     assert abs(gr.gy[0]) < 1e-6
     o = two_body((fcc.Overlap(1.0),), d=d, nθ=8000)
-    F = np.abs(o.grad.gx).max()  # gy and the torque vanish by symmetry: judge them on the force scale
+    F = np.abs(o.grad.gx).max()  # gy and the torque vanish by symmetry: measure them on the force scale
     for f in ("gx", "gy", "gθ"):
         assert np.abs(getattr(gr, f) - getattr(o.grad, f)).max() < 1e-12 * F, f
     for f in ("gcoef", "P", "GR"):

@@ -1,6 +1,6 @@
 """Host logic of the multi-GPU bench on CPU: world_size-2 `gloo` ranks.
 
-The time step does not shard (SURVEY: replicas only), so `bench.py --gpus N`
+The time step does not shard (replicas only), so `bench.py --gpus N`
 runs N independent monolayers, one per rank, with no collective in the data
 path.  What is multi-rank is the timing: the job time is the max over ranks
 and the value counts every rank's bodies.  These tests run that logic over

@@ -146,7 +146,7 @@ def test_sjf_admits_small_work_first_and_backfills():
 def test_cancelled_requests_leave_the_queue_and_the_pool():
     """A request cancelled while it runs leaves the pool with the state it
     reached; one cancelled while it waits never runs; the others are
-    unaffected (SURVEY: a cancelled request as a host-injected fault)."""
+    unaffected (a cancelled request is a fault injected on the host)."""
     clk = FakeClock()
     pool = FakePool(clk, max_bodies=160, max_sims=4)
     # r0 long and running, r1 short and running, r2 waits for room
