@@ -82,6 +82,8 @@ class Server:
                  policy="fifo", evict_ratio=4.0):
         if policy not in ("fifo", "sjf", "evict"):
             raise ArgumentError("policy must be 'fifo', 'sjf' or 'evict'")
+        if not float(evict_ratio) > 1.0:  # a ratio above 1 rules out two requests evicting each other in turn
+            raise ArgumentError("evict_ratio must be > 1")
         self.policy = policy
         self.evict_ratio = float(evict_ratio)
         self.evictions = 0

@@ -188,6 +188,8 @@ def test_evict_policy_makes_room_and_resumes_where_it_stopped():
     assert not res[0].cancelled and res[0].steps == 4000
     with pytest.raises(fcc.ArgumentError):
         fcc.Server(pool, policy="lru")
+    with pytest.raises(fcc.ArgumentError):
+        fcc.Server(pool, policy="evict", evict_ratio=1.0)
 
 
 def test_a_round_without_progress_raises_instead_of_looping():
@@ -204,3 +206,30 @@ def test_a_round_without_progress_raises_instead_of_looping():
     with pytest.raises(fcc.DeviceError):
         srv.serve([req(0, 4, 4, 100, 0.0)])
     assert srv.chunks == 1
+
+
+def test_evict_stream_neither_loses_nor_repeats_steps():
+    """A random overloaded stream under "evict": every request ends at its
+    horizon and the pool advanced each one by exactly its horizon in total
+    (an evicted request resumes where it stopped; no step is run twice)."""
+    clk = FakeClock()
+
+    class CountingPool(FakePool):
+        advanced = {}
+
+        def run(self, n):
+            for s in self.sims.values():
+                self.advanced[s["seed"]] = self.advanced.get(s["seed"], 0) + min(n, s["horizon"] - s["steps"])
+            super().run(n)
+
+    rng = np.random.default_rng(3)
+    reqs = [req(i, int(rng.integers(2, 9)), 2 * int(rng.integers(1, 5)), int(rng.integers(20, 3000)),
+                float(rng.uniform(0.0, 0.05))) for i in range(24)]
+    pool = CountingPool(clk, max_bodies=160, max_sims=3)
+    srv = fcc.Server(pool, chunk=64, min_chunk=1, clock=clk, sleep=clk.sleep, policy="evict")
+    res = srv.serve(reqs)
+    assert srv.evictions >= 1
+    assert sorted(r.id for r in res) == list(range(len(reqs)))
+    assert all(not r.cancelled and r.steps == r.horizon for r in res)
+    for q in reqs:
+        assert pool.advanced[q.kw["seed"]] == q.horizon, q.id
