@@ -233,3 +233,18 @@ def test_evict_stream_neither_loses_nor_repeats_steps():
     assert all(not r.cancelled and r.steps == r.horizon for r in res)
     for q in reqs:
         assert pool.advanced[q.kw["seed"]] == q.horizon, q.id
+
+
+def test_cancelling_an_evicted_request_reports_the_state_it_reached():
+    """An evicted request cancelled while it waits to be re-admitted is
+    reported with the state and clock it had reached, not as never run."""
+    clk = FakeClock()
+    pool = FakePool(clk, max_bodies=128, max_sims=8)
+    reqs = [req(0, 8, 12, 4000, 0.0), req(1, 8, 8, 200, 0.001)]
+    srv = fcc.Server(pool, chunk=128, min_chunk=1, clock=clk, sleep=clk.sleep, policy="evict")
+    res = {r.id: r for r in srv.serve(reqs, on_result=lambda r: srv.cancel(0) if r.id == 1 else None)}
+    assert srv.evictions == 1
+    assert not res[1].cancelled and res[1].steps == 200
+    assert res[0].cancelled and 0 < res[0].steps < 4000 and res[0].bodies is not None
+    assert res[0].admitted == 0.0
+    assert [e[1] for e in pool.log if e[0] == "add"] == [0, 1]  # never re-admitted
