@@ -133,3 +133,44 @@ def test_pool_device_bytes_without_gpu():
     assert 0 < b1 < b2 < 2 * b1 + (1 << 22) and b64 > b1
     per_body = (b2 - b1) / (1 << 20)
     assert 400 < per_body < 2000
+
+
+def _header_prototypes(path=HEADER):
+    """name -> list of parameter declarations, from the prototypes of fcc.h."""
+    text = re.sub(r"/\*.*?\*/", " ", open(path).read(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"^(?:fcc_status|const char\*)\s+(fcc_\w+)\s*\(([^)]*)\)\s*;", text, re.M):
+        params = [p.strip() for p in m.group(2).split(",") if p.strip()]
+        out[m.group(1)] = [] if params == ["void"] else params
+    return out
+
+
+def _header_kind(decl):
+    t = re.sub(r"\b\w+$", "", decl.strip()).replace("const", "").strip()  # drop the parameter name
+    if "*" in t or t == "fcc_callback":
+        return "ptr"
+    return {"int64_t": "i64", "int32_t": "i32", "uint64_t": "u64", "double": "f64", "int": "i32"}[t]
+
+
+def _ctypes_kind(t):
+    if t in (C.c_void_p, C.c_char_p) or hasattr(t, "_type_") and isinstance(t._type_, type) \
+            or getattr(t, "_flags_", 0) & C._FUNCFLAG_CDECL:
+        return "ptr"
+    return {C.c_int64: "i64", C.c_int32: "i32", C.c_uint64: "u64", C.c_double: "f64"}[t]
+
+
+def test_ctypes_signatures_match_the_header():
+    """Every argtypes list the Python mirror declares has the header's arity
+    and, parameter by parameter, the same kind (pointer, 32/64-bit integer,
+    double): a wrong width would pass values silently truncated."""
+    protos = _header_prototypes()
+    lib = fcc.simulation.native_library()  # loading and declaring need no GPU
+    fcc.pool._lib()
+    checked = 0
+    for name, params in protos.items():
+        args = getattr(lib, name).argtypes
+        if args is None:
+            continue  # not bound from Python (C and Julia callers only)
+        assert [_ctypes_kind(a) for a in args] == [_header_kind(p) for p in params], name
+        checked += 1
+    assert checked >= 30
