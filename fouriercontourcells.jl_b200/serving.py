@@ -123,32 +123,32 @@ class Server:
         waiting = deque()
         active = {}  # slot -> (request, first admitted)
         results = []
-        resume = {}  # request id -> (state, clock) of an evicted request
-        first = {}   # request id -> first admission time
+        resume = {}  # id(request) -> (state, clock) of an evicted request
+        first = {}   # id(request) -> first admission time (keyed by object: ids need not be unique)
         t0 = self.clock()
         now = lambda: self.clock() - t0
 
         def left_of(q):  # body-steps a waiting request has left
-            return q.bodies.n * (q.horizon - (resume[q.id][1] if q.id in resume else 0))
+            return q.bodies.n * (q.horizon - (resume[id(q)][1] if id(q) in resume else 0))
 
         def admit(q):
-            if q.id in resume:
-                b, c = resume[q.id]
+            if id(q) in resume:
+                b, c = resume[id(q)]
                 slot = self.pool.try_add(b, q.box, horizon=q.horizon, clock=c, **q.kw)
             else:
                 slot = self.pool.try_add(q.bodies, q.box, horizon=q.horizon, **q.kw)
             if slot is not None:
-                resume.pop(q.id, None)
-                first.setdefault(q.id, now())
-                active[slot] = (q, first[q.id])
+                resume.pop(id(q), None)
+                first.setdefault(id(q), now())
+                active[slot] = (q, first[id(q)])
             return slot
 
         while pending or waiting or active:
             ids = self._take_cancelled()
             if ids:
                 for q in [q for q in list(waiting) + list(pending) if q.id in ids]:  # not running
-                    b, c = resume.pop(q.id, (None, 0))
-                    results.append(Result(q.id, q.bodies.n, q.horizon, q.arrival, first.get(q.id, float("nan")),
+                    b, c = resume.pop(id(q), (None, 0))
+                    results.append(Result(q.id, q.bodies.n, q.horizon, q.arrival, first.get(id(q), float("nan")),
                                           now(), b, cancelled=True, steps=c))
                 waiting = deque(q for q in waiting if q.id not in ids)
                 pending = deque(q for q in pending if q.id not in ids)
@@ -177,7 +177,7 @@ class Server:
                         if work_left[s] < self.evict_ratio * left_of(r):
                             break
                         v, _ = active.pop(s)
-                        resume[v.id] = (self.pool.bodies(s), self.pool.slot(s)[1])
+                        resume[id(v)] = (self.pool.bodies(s), self.pool.slot(s)[1])
                         self.pool.remove(s)
                         self.evictions += 1
                         evicted.append(v)

@@ -248,3 +248,16 @@ def test_cancelling_an_evicted_request_reports_the_state_it_reached():
     assert res[0].cancelled and 0 < res[0].steps < 4000 and res[0].bodies is not None
     assert res[0].admitted == 0.0
     assert [e[1] for e in pool.log if e[0] == "add"] == [0, 1]  # never re-admitted
+
+
+def test_requests_without_distinct_ids_keep_their_own_admission_times():
+    """Request ids default to 0; the loop's bookkeeping is per request, so
+    a stream that leaves them all at 0 still gets each admission time right."""
+    clk = FakeClock()
+    pool = FakePool(clk, max_bodies=256, max_sims=1)
+    reqs = [fcc.Request(q.bodies, q.box, q.kw, q.horizon, q.arrival) for q in
+            (req(0, 4, 4, 100, 0.0), req(1, 4, 4, 100, 0.0), req(2, 4, 4, 100, 0.0))]
+    res = fcc.Server(pool, chunk=64, min_chunk=1, clock=clk, sleep=clk.sleep, policy="sjf").serve(reqs)
+    adm = sorted(r.admitted for r in res)
+    assert len(res) == 3 and adm[0] < adm[1] < adm[2]
+    assert all(r.admitted < r.finished for r in res)
