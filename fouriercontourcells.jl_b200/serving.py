@@ -131,13 +131,16 @@ class Server:
         def left_of(q):  # body-steps a waiting request has left
             return q.bodies.n * (q.horizon - (resume[id(q)][1] if id(q) in resume else 0))
 
+        steps_now = {}  # slot -> steps done, read once per admission pass (steps change only in runs)
+
         def admit(q):
-            if id(q) in resume:
-                b, c = resume[id(q)]
+            b, c = resume.get(id(q), (q.bodies, 0))
+            if c:
                 slot = self.pool.try_add(b, q.box, horizon=q.horizon, clock=c, **q.kw)
             else:
-                slot = self.pool.try_add(q.bodies, q.box, horizon=q.horizon, **q.kw)
+                slot = self.pool.try_add(b, q.box, horizon=q.horizon, **q.kw)
             if slot is not None:
+                steps_now[slot] = c
                 resume.pop(id(q), None)
                 first.setdefault(id(q), now())
                 active[slot] = (q, first[id(q)])
@@ -169,15 +172,18 @@ class Server:
                     waiting.popleft()
             else:  # least work left first; every waiting request that fits is admitted
                 admitted, evicted = set(), []
+                if self.policy == "evict" and waiting:
+                    steps_now.clear()
+                    steps_now.update((s, self.pool.slot(s)[1]) for s in active)
                 for r in sorted(waiting, key=lambda q: (left_of(q), q.arrival)):
                     slot = admit(r)
                     while slot is None and self.policy == "evict" and active:
-                        work_left = {s: v.bodies.n * (v.horizon - self.pool.slot(s)[1]) for s, (v, _) in active.items()}
+                        work_left = {s: v.bodies.n * (v.horizon - steps_now[s]) for s, (v, _) in active.items()}
                         s = max(work_left, key=work_left.get)
                         if work_left[s] < self.evict_ratio * left_of(r):
                             break
                         v, _ = active.pop(s)
-                        resume[id(v)] = (self.pool.bodies(s), self.pool.slot(s)[1])
+                        resume[id(v)] = (self.pool.bodies(s), steps_now.pop(s))
                         self.pool.remove(s)
                         self.evictions += 1
                         evicted.append(v)
