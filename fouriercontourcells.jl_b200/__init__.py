@@ -19,7 +19,8 @@ from .model import (ArgumentError, DimensionMismatch, DeviceError, PoolFull, Bod
                     polydisperse_monolayer, minimum_image, wrap)
 from .simulation import (Simulation, NativeSimulation, native_library, step, run, compute_gradients,
                          update_neighbors, perimeters, areas, shape_index, body_energy, positions,
-                         unwrapped_positions, contours, protrusion, Gradients, Geometry, NeighborInfo)
+                         unwrapped_positions, contours, protrusion, Gradients, Geometry, NeighborInfo,
+                         pinned_bodies, pinned_copy)
 from .ops import philox_noise, build_neighbors, barrier_selftest
 from .pool import Pool
 from .serving import Request, Result, Server
@@ -31,5 +32,5 @@ __all__ = [
     "polydisperse_monolayer", "minimum_image", "wrap", "Simulation", "NativeSimulation", "native_library", "step",
     "run", "compute_gradients", "update_neighbors", "perimeters", "areas", "shape_index", "body_energy",
     "positions", "unwrapped_positions", "contours", "protrusion", "Gradients", "Geometry", "NeighborInfo",
-    "philox_noise", "build_neighbors", "barrier_selftest",
+    "philox_noise", "build_neighbors", "barrier_selftest", "pinned_bodies", "pinned_copy",
 ]

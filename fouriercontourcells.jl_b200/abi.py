@@ -172,7 +172,12 @@ class ParamsBuffer:
 
 
 class BodiesBuffer:
-    """Contiguous numpy arrays behind an ``fcc_bodies_host`` (column-major coef)."""
+    """Contiguous numpy arrays behind an ``fcc_bodies_host``.
+
+    ``coef`` is ``ncoef × N`` in Fortran (column-major) order, as Julia
+    stores it: one body's coefficients are contiguous, which is the ABI's
+    layout, so ``coefT`` (``N × ncoef``, C order) is a view of the same
+    memory."""
 
     def __init__(self, n: int, ncoef: int):
         self.n, self.ncoef = n, ncoef
@@ -181,7 +186,6 @@ class BodiesBuffer:
         self.theta = np.zeros(n)
         self.imgx = np.zeros(n, np.int32)
         self.imgy = np.zeros(n, np.int32)
-        # (N, ncoef) C-order == ncoef x N column-major
         self.coefT = np.zeros((n, ncoef))
         self.R0 = np.zeros(n)
         self.type = np.zeros(n, np.int32)
@@ -192,20 +196,80 @@ class BodiesBuffer:
     @classmethod
     def from_bodies(cls, b: Bodies):
         buf = cls(b.n, b.ncoef)
-        buf.x[:] = b.x
-        buf.y[:] = b.y
-        buf.theta[:] = b.θ
-        buf.imgx[:] = b.imgx
-        buf.imgy[:] = b.imgy
-        buf.coefT[:] = np.asarray(b.coef).T
-        buf.R0[:] = b.R0
-        buf.type[:] = b.type
-        buf.parent[:] = b.parent
+        buf.fill(b)
         return buf
+
+    def fill(self, b: Bodies):
+        self.x[:] = b.x
+        self.y[:] = b.y
+        self.theta[:] = b.θ
+        self.imgx[:] = b.imgx
+        self.imgy[:] = b.imgy
+        self.coefT[:] = np.asarray(b.coef).T
+        self.R0[:] = b.R0
+        self.type[:] = b.type
+        self.parent[:] = b.parent
 
     def to_bodies(self) -> Bodies:
         return Bodies(self.x.copy(), self.y.copy(), self.theta.copy(), self.imgx.copy(), self.imgy.copy(),
-                      self.coefT.T.copy(), self.R0.copy(), self.type.copy(), self.parent.copy())
+                      self.coefT.copy().T, self.R0.copy(), self.type.copy(), self.parent.copy())
+
+
+def _flat(a, dtype, writable):
+    """`a` itself if it is a contiguous 1-d array of `dtype` (writable when
+    asked), else None."""
+    if (isinstance(a, np.ndarray) and a.dtype == dtype and a.ndim == 1 and a.flags.c_contiguous
+            and (a.flags.writeable or not writable)):
+        return a
+    return None
+
+
+def direct_host(b: Bodies, writable: bool = False):
+    """An ``fcc_bodies_host`` over the arrays of `b` themselves, or None when
+    one of them is not already in the ABI's layout (contiguous float64 /
+    int32 vectors, ``coef`` ``ncoef × N`` in Fortran order).  The library
+    then reads (set_state) or writes (get_state) them in place with one copy
+    each to or from the device — a DMA when they are pinned."""
+    n = b.n
+    f = {k: _flat(getattr(b, a), dt, writable) for k, a, dt in (
+        ("x", "x", np.float64), ("y", "y", np.float64), ("theta", "θ", np.float64), ("imgx", "imgx", np.int32),
+        ("imgy", "imgy", np.int32), ("R0", "R0", np.float64), ("type", "type", np.int32),
+        ("parent", "parent", np.int32))}
+    c = b.coef
+    if (any(v is None or len(v) != n for v in f.values()) or not isinstance(c, np.ndarray) or c.dtype != np.float64
+            or c.ndim != 2 or c.shape[1] != n or not c.flags.f_contiguous or (writable and not c.flags.writeable)):
+        return None
+    return FccBodiesHost(n, c.shape[0], dptr(f["x"]), dptr(f["y"]), dptr(f["theta"]), iptr(f["imgx"]),
+                         iptr(f["imgy"]), c.ctypes.data_as(c_double_p), dptr(f["R0"]), iptr(f["type"]),
+                         iptr(f["parent"]))
+
+
+def bodies_over(block: np.ndarray, n: int, ncoef: int) -> Bodies:
+    """A ``Bodies`` whose arrays are views into one uint8 `block` of at least
+    ``bodies_bytes(n, ncoef)`` bytes, every array 64-byte aligned and in the
+    ABI's layout (so ``direct_host`` takes it as it is)."""
+    views, off = {}, 0
+    base = block.ctypes.data
+
+    def take(name, dtype, count):
+        nonlocal off
+        off += (-(base + off)) % 64
+        nb = count * np.dtype(dtype).itemsize
+        views[name] = block[off:off + nb].view(dtype)
+        off += nb
+
+    for name, dt in (("x", np.float64), ("y", np.float64), ("θ", np.float64), ("R0", np.float64)):
+        take(name, dt, n)
+    for name in ("imgx", "imgy", "type", "parent"):
+        take(name, np.int32, n)
+    take("coef", np.float64, n * ncoef)
+    views["coef"] = views["coef"].reshape(n, ncoef).T
+    return Bodies(**views)
+
+
+def bodies_bytes(n: int, ncoef: int) -> int:
+    """Bytes ``bodies_over`` needs (with room for the 64-byte alignment)."""
+    return 8 * n * (4 + ncoef) + 4 * 4 * n + 9 * 64
 
 
 def check(status: int, lasterr) -> None:

@@ -1739,10 +1739,15 @@ __global__ void k_finish_rebuild(DevPtrs<T> d) {
 // Simulation set-up and set_state: enforce_shape! (FP64 sums) and the lab
 // frame of the given body state into rec[par] (src/simulation.jl:102-103,
 // src/dynamics.jl:44-64, src/geometry.jl:208-227).  One thread per body.
-// Bodies g0 .. g0+n-1; the inputs are indexed from g0.
+// Bodies g0 .. g0+n-1; the inputs are indexed from i = 0 and are the caller's
+// host values as they crossed the ABI (double), in the reference's
+// coefficient layout: in_nc values per body, [a0; a_2..a_{in_K+1};
+// b_2..b_{in_K+1}] (src/basis.jl:10-14).  Each value is rounded to T here,
+// exactly as a host-side conversion would round it.
 template <class T>
-__global__ void k_init(DevPtrs<T> d, int par, int g0, int n, const T* __restrict__ x, const T* __restrict__ y,
-                       const T* __restrict__ th, const T* __restrict__ coef_in) {
+__global__ void k_init(DevPtrs<T> d, int par, int g0, int n, const double* __restrict__ x,
+                       const double* __restrict__ y, const double* __restrict__ th_in,
+                       const double* __restrict__ coef_in, int in_nc, int in_K) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int g = g0 + i;
@@ -1750,8 +1755,14 @@ __global__ void k_init(DevPtrs<T> d, int par, int g0, int n, const T* __restrict
     const SimDesc<T>& P = d.sims[s];
     const int K = P.K;
     T c[NCM];
+    const double* ci = coef_in + (size_t)i * in_nc;
+    c[0] = T(ci[0]);
 #pragma unroll
-    for (int r = 0; r < NCM; ++r) c[r] = coef_in[(size_t)i * NCM + r];
+    for (int m = 0; m < KM; ++m) {
+        c[1 + m] = m < in_K ? T(ci[1 + m]) : T(0);
+        c[1 + KM + m] = m < in_K ? T(ci[1 + in_K + m]) : T(0);
+    }
+    const T th_i = T(th_in[i]);
     // enforce_shape! and the lab frame with the arithmetic of the update's
     // end of step (update_body): modes spread over 8 lanes as m = lane + 8u,
     // per-lane sums in u order, lanes combined by the xor butterfly of
@@ -1797,7 +1808,7 @@ __global__ void k_init(DevPtrs<T> d, int par, int g0, int n, const T* __restrict
     T* ro = rec_next(d, par) + (size_t)g * RECW;
     for (int r = 0; r < RECW; ++r) ro[r] = T(0);
     T s1, c1;
-    t_sincos(th[i], &s1, &c1);
+    t_sincos(th_i, &s1, &c1);
     T bpl[LV];
 #pragma unroll
     for (int l = 0; l < LV; ++l) {
@@ -1819,11 +1830,11 @@ __global__ void k_init(DevPtrs<T> d, int par, int g0, int n, const T* __restrict
         bpl[l] = bp;
     }
     const T bound = c[0] + tree8(bpl);
-    rn[R_X] = x[i];
-    rn[R_Y] = y[i];
+    rn[R_X] = T(x[i]);
+    rn[R_Y] = T(y[i]);
     rn[R_RMAX] = r0 * bound;
     rn[R_A0] = r0 * c[0];  // R_W (parent, type) is written by k_set_w
-    rn[R_TH] = th[i];
+    rn[R_TH] = th_i;
 #pragma unroll
     for (int r = 0; r < NCM; ++r) d.coef[(size_t)g * NCM + r] = c[r];
 }
@@ -1835,6 +1846,30 @@ __global__ void k_set_w(DevPtrs<T> d, int par, int g0, int n, const int* __restr
     if (i >= n) return;
     T* tag = nullptr;
     rec_cur_mut(d, par)[(size_t)(g0 + i) * RECW + R_W] = pack_w(w[i], tag);
+}
+
+// get_state on the device: x, y, theta of the current record and the
+// body-frame coefficients of bodies g0 .. g0+n-1, widened to double in the
+// reference's layout (xyt: x[n], y[n], theta[n]; coef_out: out_nc values per
+// body, [a0; a_2..a_{out_K+1}; b_2..b_{out_K+1}]), ready to be copied to the
+// caller's host arrays as they are.
+template <class T>
+__global__ void k_store_host(DevPtrs<T> d, int par, int g0, int n, double* __restrict__ xyt,
+                             double* __restrict__ coef_out, int out_nc, int out_K) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int g = g0 + i;
+    const T* rc = rec_cur(d, par) + (size_t)g * RECW;
+    xyt[i] = (double)rc[R_X];
+    xyt[(size_t)n + i] = (double)rc[R_Y];
+    xyt[2 * (size_t)n + i] = (double)rc[R_TH];
+    const T* cf = d.coef + (size_t)g * NCM;
+    double* co = coef_out + (size_t)i * out_nc;
+    co[0] = (double)cf[0];
+    for (int m = 0; m < out_K; ++m) {
+        co[1 + m] = (double)cf[1 + m];
+        co[1 + out_K + m] = (double)cf[1 + KM + m];
+    }
 }
 
 // Geometry of the current state for get_geometry: lab, labR0, rmax, and

@@ -112,8 +112,12 @@ template <class V>
 struct Stage {
     DBuf<V> buf;
     fcc_status upload(const std::vector<V>& h, cudaStream_t st) {
-        if (h.size() > buf.n) FCC_TRY(buf.alloc(h.size(), st));
+        FCC_TRY(reserve(h.size(), st));
         if (!h.empty()) CUDA_TRY(cudaMemcpyAsync(buf.p, h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice, st));
+        return FCC_OK;
+    }
+    fcc_status reserve(size_t count, cudaStream_t st) {
+        if (count > buf.n) FCC_TRY(buf.alloc(count, st));
         return FCC_OK;
     }
     V* p() const { return buf.p; }
@@ -507,18 +511,17 @@ struct Engine final : EngineBase {
         GridSync sync;
     };
     Status* st_h = nullptr;
-    // state exchange with the host (set_state / get_state): one pinned host
-    // area and one device area, allocated at the first exchange and reused,
-    // so that no call after the first allocates, frees or copies pageable memory
-    void* xch_h = nullptr;
-    size_t xch_bytes = 0;
-    DBuf<T> xch_t;
-    DBuf<int> xch_w;
+    // state exchange with the host (set_state / get_state): the caller's
+    // double arrays are copied as they are into one device area (x, y, theta,
+    // coefficients in the reference's layout), and converted and repacked on
+    // the device; allocated at create and reused, so no exchange allocates.
+    // w_dev holds the (parent, type) record words, fixed since create.
+    DBuf<double> xch_d;
+    DBuf<int> w_dev;
 
     ~Engine() override {
         if (stream) cudaStreamSynchronize(stream);
         if (st_h) cudaFreeHost(st_h);
-        if (xch_h) cudaFreeHost(xch_h);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -657,6 +660,11 @@ struct Engine final : EngineBase {
         FCC_TRY(builds.alloc(1, stream));
         FCC_TRY(sync.alloc(1, stream));
 
+        std::vector<int> w(n);
+        for (size_t i = 0; i < n; ++i) w[i] = ((parent_h[i] - 1) << 3) | (type_h[i] - 1);
+        FCC_TRY(w_dev.upload(w, stream));
+        FCC_TRY(xch_d.alloc(n * (3 + (size_t)nc), stream));
+
         // launch configuration of the persistent kernel: all co-resident blocks
         FCC_TRY(configure());
         FCC_TRY(load_state(b, 0));
@@ -747,59 +755,22 @@ struct Engine final : EngineBase {
     }
 
     // Copy a host body state in and rebuild the derived geometry (k_init).
-    // Pinned host area of the state exchange, per body: 3 + NCM + RECW T values
-    // and 3 ints.  set_state stages x, y, theta, the coefficients, the w word
-    // and the image counts; get_state reads back the record, the coefficients
-    // and the image counts.
-    fcc_status exchange_area() {
-        const size_t n = (size_t)N;
-        const size_t bytes = n * ((3 + NCM + RECW) * sizeof(T) + 3 * sizeof(int));
-        if (bytes && !(xch_h && xch_bytes >= bytes)) {
-            if (xch_h) cudaFreeHost(xch_h);
-            xch_h = nullptr;
-            xch_bytes = 0;
-            CUDA_TRY(cudaMallocHost(&xch_h, bytes));
-            xch_bytes = bytes;
-        }
-        if (xch_t.n != n * (3 + NCM)) FCC_TRY(xch_t.alloc(n * (3 + NCM), stream));
-        if (xch_w.n != n) FCC_TRY(xch_w.alloc(n, stream));
-        return FCC_OK;
-    }
-    T* xch_tvals() const { return (T*)xch_h; }
-    int* xch_ints() const { return (int*)((T*)xch_h + (size_t)N * (3 + NCM + RECW)); }
-
+    // The caller's arrays go to the device as they are (a DMA when the caller
+    // passes pinned host memory; the driver stages pageable memory), and
+    // k_init rounds them to T and repacks the coefficients, so the host does
+    // no per-body work.  The call returns once the copies have completed: the
+    // caller may reuse its buffers.
     fcc_status load_state(const fcc_bodies_host* b, int64_t clk) {
         const size_t n = (size_t)N;
-        FCC_TRY(exchange_area());
-        T* hx = xch_tvals();
-        T* hy = hx + n;
-        T* hth = hy + n;
-        T* hc = hth + n;
-        int* w = xch_ints();
-        int* ix = w + n;
-        int* iy = ix + n;
-        for (size_t i = 0; i < n; ++i) {
-            hx[i] = (T)b->x[i];
-            hy[i] = (T)b->y[i];
-            hth[i] = (T)b->theta[i];
-            const double* c = b->coef + i * nc;
-            T* r = hc + i * NCM;
-            for (int m = 0; m < NCM; ++m) r[m] = T(0);
-            r[0] = (T)c[0];
-            for (int m = 0; m < K; ++m) {
-                r[1 + m] = (T)c[1 + m];
-                r[1 + KM + m] = (T)c[1 + K + m];
-            }
-            w[i] = ((parent_h[i] - 1) << 3) | (type_h[i] - 1);
-            if (b->imgx) ix[i] = b->imgx[i];
-            if (b->imgy) iy[i] = b->imgy[i];
-        }
         if (clk >= 0) clock_h = clk;
+        double* dx = xch_d.p;
         if (n) {
-            CUDA_TRY(cudaMemcpyAsync(xch_t.p, hx, n * (3 + NCM) * sizeof(T), cudaMemcpyHostToDevice, stream));
-            CUDA_TRY(cudaMemcpyAsync(xch_w.p, w, n * sizeof(int), cudaMemcpyHostToDevice, stream));
-            if (b->imgx) CUDA_TRY(cudaMemcpyAsync(imgx.p, ix, n * sizeof(int), cudaMemcpyHostToDevice, stream));
-            if (b->imgy) CUDA_TRY(cudaMemcpyAsync(imgy.p, iy, n * sizeof(int), cudaMemcpyHostToDevice, stream));
+            CUDA_TRY(cudaMemcpyAsync(dx, b->x, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+            CUDA_TRY(cudaMemcpyAsync(dx + n, b->y, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+            CUDA_TRY(cudaMemcpyAsync(dx + 2 * n, b->theta, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+            CUDA_TRY(cudaMemcpyAsync(dx + 3 * n, b->coef, n * nc * sizeof(double), cudaMemcpyHostToDevice, stream));
+            if (b->imgx) CUDA_TRY(cudaMemcpyAsync(imgx.p, b->imgx, n * sizeof(int), cudaMemcpyHostToDevice, stream));
+            if (b->imgy) CUDA_TRY(cudaMemcpyAsync(imgy.p, b->imgy, n * sizeof(int), cudaMemcpyHostToDevice, stream));
             CUDA_TRY(cudaMemsetAsync(sim_of.p, 0, n * sizeof(int), stream));
         }
         CUDA_TRY(cudaMemcpyAsync(clock.p, &clock_h, sizeof(long long), cudaMemcpyHostToDevice, stream));
@@ -807,10 +778,9 @@ struct Engine final : EngineBase {
         const DevPtrs<T> d = ptrs();
         if (N > 0) {
             const int grid = (int)((N + 255) / 256);
-            const T* dx = xch_t.p;
-            k_init<T><<<grid, 256, 0, stream>>>(d, par(), 0, (int)N, dx, dx + n, dx + 2 * n, dx + 3 * n);
+            k_init<T><<<grid, 256, 0, stream>>>(d, par(), 0, (int)N, dx, dx + n, dx + 2 * n, dx + 3 * n, nc, K);
             CUDA_TRY(cudaGetLastError());
-            k_set_w<T><<<grid, 256, 0, stream>>>(d, par(), 0, (int)N, xch_w.p);
+            k_set_w<T><<<grid, 256, 0, stream>>>(d, par(), 0, (int)N, w_dev.p);
             CUDA_TRY(cudaGetLastError());
         }
         // list invalid: the next step (or update_neighbors!) rebuilds
@@ -818,7 +788,7 @@ struct Engine final : EngineBase {
         CUDA_TRY(cudaMemcpyAsync(flags.p, &f, sizeof(int), cudaMemcpyHostToDevice, stream));
         GridSync gs{0, 0, 0, has_contact ? 1 : 0};
         CUDA_TRY(cudaMemcpyAsync(sync.p, &gs, sizeof(GridSync), cudaMemcpyHostToDevice, stream));
-        return sync_stream();  // the exchange area is free for the next call on return
+        return sync_stream();  // the caller's arrays are free for reuse on return
     }
 
     int par() const { return (int)(gstep & 1); }
@@ -1002,33 +972,36 @@ struct Engine final : EngineBase {
         return FCC_OK;
     }
 
+    // sim.bodies: k_store_host widens x, y, theta and the coefficients to
+    // double in the reference's layout on the device; they and the image
+    // counters are copied straight into the caller's arrays (a DMA for pinned
+    // host memory).  R0, type and parent are fixed since create and come from
+    // the host mirror.
     fcc_status get_state(fcc_bodies_host* o, int64_t* clk, double* t, int64_t* stp) override {
         if (o) {
             if (o->n != N || o->ncoef != nc) return fail(FCC_ERR_DIMENSION, "state buffers do not match the simulation");
             const size_t n = (size_t)N;
-            FCC_TRY(exchange_area());
-            T* cf = xch_tvals();
-            T* rec = cf + n * NCM;
-            int* ix = xch_ints();
-            int* iy = ix + n;
             if (n) {
-                CUDA_TRY(cudaMemcpyAsync(rec, par() ? rec1.p : rec0.p, n * RECW * sizeof(T), cudaMemcpyDeviceToHost, stream));
-                CUDA_TRY(cudaMemcpyAsync(cf, coef.p, n * NCM * sizeof(T), cudaMemcpyDeviceToHost, stream));
-                CUDA_TRY(cudaMemcpyAsync(ix, imgx.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
-                CUDA_TRY(cudaMemcpyAsync(iy, imgy.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+                double* dx = xch_d.p;
+                const int grid = (int)((N + 255) / 256);
+                k_store_host<T><<<grid, 256, 0, stream>>>(ptrs(), par(), 0, (int)N, dx, dx + 3 * n, nc, K);
+                CUDA_TRY(cudaGetLastError());
+                if (o->x) CUDA_TRY(cudaMemcpyAsync(o->x, dx, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+                if (o->y) CUDA_TRY(cudaMemcpyAsync(o->y, dx + n, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+                if (o->theta)
+                    CUDA_TRY(cudaMemcpyAsync(o->theta, dx + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+                if (o->coef)
+                    CUDA_TRY(cudaMemcpyAsync(o->coef, dx + 3 * n, n * nc * sizeof(double), cudaMemcpyDeviceToHost, stream));
+                if (o->imgx) CUDA_TRY(cudaMemcpyAsync(o->imgx, imgx.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+                if (o->imgy) CUDA_TRY(cudaMemcpyAsync(o->imgy, imgy.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
             }
-            FCC_TRY(sync_stream());
-            for (int64_t i = 0; i < N; ++i) {
-                if (o->x) o->x[i] = (double)rec[(size_t)i * RECW + R_X];
-                if (o->y) o->y[i] = (double)rec[(size_t)i * RECW + R_Y];
-                if (o->theta) o->theta[i] = (double)rec[(size_t)i * RECW + R_TH];
-                if (o->imgx) o->imgx[i] = ix[i];
-                if (o->imgy) o->imgy[i] = iy[i];
+            // the fixed fields while the copies run
+            for (size_t i = 0; i < n; ++i) {
                 if (o->R0) o->R0[i] = (double)R0_h[i];
                 if (o->type) o->type[i] = type_h[i];
                 if (o->parent) o->parent[i] = parent_h[i];
             }
-            if (o->coef) coef_out(cf, o->coef);
+            FCC_TRY(sync_stream());
         }
         if (clk) *clk = clock_h;
         if (t) *t = (double)t_h;
@@ -1405,6 +1378,17 @@ fcc_status fcc_get_state(fcc_sim* sim, fcc_bodies_host* out, int64_t* clock, dou
 }
 fcc_status fcc_set_state(fcc_sim* sim, const fcc_bodies_host* in, int64_t clock) { SIM_CALL(set_state(in, clock)); }
 fcc_status fcc_set_dt(fcc_sim* sim, double dt) { SIM_CALL(set_dt(dt)); }
+fcc_status fcc_host_alloc(int64_t bytes, void** out) {
+    if (!out || bytes < 0) return fail(FCC_ERR_ARGUMENT, "fcc_host_alloc: bad argument");
+    *out = nullptr;
+    if (bytes == 0) return FCC_OK;
+    CUDA_TRY(cudaMallocHost(out, (size_t)bytes));
+    return FCC_OK;
+}
+fcc_status fcc_host_free(void* ptr) {
+    if (ptr) CUDA_TRY(cudaFreeHost(ptr));
+    return FCC_OK;
+}
 fcc_status fcc_get_gradients(fcc_sim* sim, const fcc_gradients_host* out) { SIM_CALL(get_gradients(out)); }
 fcc_status fcc_get_geometry(fcc_sim* sim, const fcc_geometry_host* out) { SIM_CALL(get_geometry(out)); }
 fcc_status fcc_neighbor_dims(fcc_sim* sim, int32_t* ncx, int32_t* ncy, int32_t* cap, int64_t* builds, int32_t* valid) {

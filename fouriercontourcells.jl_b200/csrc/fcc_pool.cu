@@ -189,7 +189,7 @@ __global__ void k_pool_slot_ids(int* sim_of, int* cell_sim, int* ch_count, int* 
 
 struct PoolBase {
     virtual ~PoolBase() = default;
-    virtual fcc_status add(const fcc_params* p, const fcc_bodies_host* b, int64_t horizon, int64_t clock0,
+    virtual fcc_status add(const fcc_params* p, const fcc_bodies_host* b, int64_t horizon, int64_t clock0, double t0,
                            int32_t* slot) = 0;
     virtual fcc_status remove(int32_t slot) = 0;
     virtual fcc_status run(int64_t n) = 0;
@@ -233,7 +233,7 @@ struct Pool final : PoolBase {
     DBuf<MoveRange> moves;
     std::vector<SimDesc<T>> desc_stage;  // host staging of the descriptors a compaction rebases
     // device staging of an admission (bodies, child and bond lists), reused
-    Stage<T> st_x, st_y, st_th, st_c;
+    Stage<double> st_xch;  // host state exchange: x, y, theta, coefficients as the caller's doubles
     Stage<int> st_w, st_chc, st_chi, st_bdc, st_bdi;
     ObsArea obs;  // perimeters / areas / shape indices: reused device and pinned host buffers
 
@@ -408,11 +408,12 @@ struct Pool final : PoolBase {
     }
 
     // ------------------------------------------------------- admission --
-    fcc_status add(const fcc_params* p, const fcc_bodies_host* b, int64_t horizon, int64_t clock0,
+    fcc_status add(const fcc_params* p, const fcc_bodies_host* b, int64_t horizon, int64_t clock0, double t0,
                    int32_t* slot_out) override {
         Range range("fcc pool add");
         if (!p || !b || !slot_out) return fail(FCC_ERR_ARGUMENT, "null argument");
         if (clock0 < 0) return fail(FCC_ERR_ARGUMENT, "pool: clock must be >= 0");
+        if (std::isnan(t0)) return fail(FCC_ERR_ARGUMENT, "pool: t must not be NaN");
         if (p->precision != (sizeof(T) == 4 ? 32 : 64))
             return fail(FCC_ERR_ARGUMENT, "pool: the simulation's precision differs from the pool's");
         if (p->ntheta != nth) return fail(FCC_ERR_DIMENSION, "pool: the simulation's ntheta differs from the pool's");
@@ -445,11 +446,13 @@ struct Pool final : PoolBase {
         S.coff = (int)Ctot;
         S.ncells = (int)nce;
         S.horizon = horizon;
-        // a resumed simulation counts its steps (and time) from its clock, so
-        // that steps done and the horizon are both measured on the clock
+        // a resumed simulation counts its steps from its clock, so that steps
+        // done and the horizon are both measured on the clock; its time is the
+        // checkpoint's (t0), or clock * dt when the caller has none (t0 < 0:
+        // exact only if dt never changed before the checkpoint)
         S.clock_h = clock0;
         S.step_h = clock0;
-        S.t_h = (T)((double)clock0 * (double)sp.desc.dt);
+        S.t_h = t0 >= 0 ? (T)t0 : (T)((double)clock0 * (double)sp.desc.dt);
         sp.desc.body_off = (int)S.off;
         sp.desc.cell_off = S.coff;
         S.spec = std::move(sp);
@@ -495,34 +498,27 @@ struct Pool final : PoolBase {
         return sync_stream();
     }
 
-    // enforce_shape! and lab frame of a slot's host state (k_init, k_set_w)
+    // enforce_shape! and lab frame of a slot's host state (k_init, k_set_w):
+    // the caller's double arrays are copied as they are and converted on the
+    // device
     fcc_status load_bodies(int s, const fcc_bodies_host* b) {
         Slot& S = slots[s];
         const SimSpec<T>& P = S.spec;
         const size_t n = (size_t)P.N;
         if (n == 0) return FCC_OK;
-        std::vector<T> hx(n), hy(n), hth(n), hc(n * NCM, T(0));
         std::vector<int> w(n);
-        for (size_t i = 0; i < n; ++i) {
-            hx[i] = (T)b->x[i];
-            hy[i] = (T)b->y[i];
-            hth[i] = (T)b->theta[i];
-            const double* c = b->coef + i * P.nc;
-            hc[i * NCM] = (T)c[0];
-            for (int m = 0; m < P.K; ++m) {
-                hc[i * NCM + 1 + m] = (T)c[1 + m];
-                hc[i * NCM + 1 + KM + m] = (T)c[1 + P.K + m];
-            }
-            w[i] = (((int)S.off + P.parent[i] - 1) << 3) | (P.type[i] - 1);
-        }
-        FCC_TRY(st_x.upload(hx, stream));
-        FCC_TRY(st_y.upload(hy, stream));
-        FCC_TRY(st_th.upload(hth, stream));
-        FCC_TRY(st_c.upload(hc, stream));
+        for (size_t i = 0; i < n; ++i) w[i] = (((int)S.off + P.parent[i] - 1) << 3) | (P.type[i] - 1);
+        FCC_TRY(st_xch.reserve(n * (3 + (size_t)P.nc), stream));
+        double* dx = st_xch.p();
+        CUDA_TRY(cudaMemcpyAsync(dx, b->x, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(cudaMemcpyAsync(dx + n, b->y, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(cudaMemcpyAsync(dx + 2 * n, b->theta, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(cudaMemcpyAsync(dx + 3 * n, b->coef, n * P.nc * sizeof(double), cudaMemcpyHostToDevice, stream));
         FCC_TRY(st_w.upload(w, stream));
         const DevPtrs<T> d = ptrs();
         const int blocks = (int)((n + 255) / 256);
-        k_init<T><<<blocks, 256, 0, stream>>>(d, par(), (int)S.off, (int)n, st_x.p(), st_y.p(), st_th.p(), st_c.p());
+        k_init<T><<<blocks, 256, 0, stream>>>(d, par(), (int)S.off, (int)n, dx, dx + n, dx + 2 * n, dx + 3 * n, P.nc,
+                                              P.K);
         CUDA_TRY(cudaGetLastError());
         k_set_w<T><<<blocks, 256, 0, stream>>>(d, par(), (int)S.off, (int)n, st_w.p());
         CUDA_TRY(cudaGetLastError());
@@ -1004,34 +1000,31 @@ struct Pool final : PoolBase {
         if (o) {
             if (o->n != N || o->ncoef != P.nc) return fail(FCC_ERR_DIMENSION, "state buffers do not match the simulation");
             Arena<T>& a = *A;
-            std::vector<T> rec((size_t)N * RECW), cf((size_t)N * NCM);
-            std::vector<int> ix(N), iy(N);
-            if (N > 0) {
-                const T* rc = par() ? a.rec1.p : a.rec0.p;
-                CUDA_TRY(cudaMemcpyAsync(rec.data(), rc + (size_t)S.off * RECW, rec.size() * sizeof(T), cudaMemcpyDeviceToHost, stream));
-                CUDA_TRY(cudaMemcpyAsync(cf.data(), a.coef.p + (size_t)S.off * NCM, cf.size() * sizeof(T), cudaMemcpyDeviceToHost, stream));
-                CUDA_TRY(cudaMemcpyAsync(ix.data(), a.imgx.p + S.off, N * sizeof(int), cudaMemcpyDeviceToHost, stream));
-                CUDA_TRY(cudaMemcpyAsync(iy.data(), a.imgy.p + S.off, N * sizeof(int), cudaMemcpyDeviceToHost, stream));
-                FCC_TRY(sync_stream());
+            const size_t n = (size_t)N;
+            if (n > 0) {
+                FCC_TRY(st_xch.reserve(n * (3 + (size_t)P.nc), stream));
+                double* dx = st_xch.p();
+                k_store_host<T><<<(int)((n + 255) / 256), 256, 0, stream>>>(ptrs(), par(), (int)S.off, (int)n, dx,
+                                                                            dx + 3 * n, P.nc, P.K);
+                CUDA_TRY(cudaGetLastError());
+                if (o->x) CUDA_TRY(cudaMemcpyAsync(o->x, dx, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+                if (o->y) CUDA_TRY(cudaMemcpyAsync(o->y, dx + n, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+                if (o->theta)
+                    CUDA_TRY(cudaMemcpyAsync(o->theta, dx + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+                if (o->coef)
+                    CUDA_TRY(cudaMemcpyAsync(o->coef, dx + 3 * n, n * P.nc * sizeof(double), cudaMemcpyDeviceToHost,
+                                             stream));
+                if (o->imgx)
+                    CUDA_TRY(cudaMemcpyAsync(o->imgx, a.imgx.p + S.off, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+                if (o->imgy)
+                    CUDA_TRY(cudaMemcpyAsync(o->imgy, a.imgy.p + S.off, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
             }
-            for (int64_t i = 0; i < N; ++i) {
-                if (o->x) o->x[i] = (double)rec[(size_t)i * RECW + R_X];
-                if (o->y) o->y[i] = (double)rec[(size_t)i * RECW + R_Y];
-                if (o->theta) o->theta[i] = (double)rec[(size_t)i * RECW + R_TH];
-                if (o->imgx) o->imgx[i] = ix[i];
-                if (o->imgy) o->imgy[i] = iy[i];
+            for (size_t i = 0; i < n; ++i) {
                 if (o->R0) o->R0[i] = (double)P.R0[i];
                 if (o->type) o->type[i] = P.type[i];
                 if (o->parent) o->parent[i] = P.parent[i];
-                if (o->coef) {
-                    double* dst = o->coef + (size_t)i * P.nc;
-                    dst[0] = (double)cf[(size_t)i * NCM];
-                    for (int m = 0; m < P.K; ++m) {
-                        dst[1 + m] = (double)cf[(size_t)i * NCM + 1 + m];
-                        dst[1 + P.K + m] = (double)cf[(size_t)i * NCM + 1 + KM + m];
-                    }
-                }
             }
+            FCC_TRY(sync_stream());
         }
         if (clk) *clk = S.clock_h;
         if (t) *t = (double)S.t_h;
@@ -1159,11 +1152,11 @@ fcc_status fcc_pool_destroy(fcc_pool* pool) {
 
 fcc_status fcc_pool_add(fcc_pool* pool, const fcc_params* params, const fcc_bodies_host* bodies, int64_t horizon,
                         int32_t* slot) {
-    POOL_CALL(add(params, bodies, horizon, 0, slot));
+    POOL_CALL(add(params, bodies, horizon, 0, 0.0, slot));
 }
 fcc_status fcc_pool_add_at(fcc_pool* pool, const fcc_params* params, const fcc_bodies_host* bodies, int64_t clock,
-                           int64_t horizon, int32_t* slot) {
-    POOL_CALL(add(params, bodies, horizon, clock, slot));
+                           double t, int64_t horizon, int32_t* slot) {
+    POOL_CALL(add(params, bodies, horizon, clock, t, slot));
 }
 fcc_status fcc_pool_remove(fcc_pool* pool, int32_t slot) { POOL_CALL(remove(slot)); }
 fcc_status fcc_pool_run(fcc_pool* pool, int64_t n) { POOL_CALL(run(n)); }

@@ -233,8 +233,9 @@ def wrap(x, L):
 class Bodies:
     """Structure-of-arrays body state (src/bodies.jl:62-86).
 
-    ``coef`` is ``ncoef × N`` (column i = [a0; a2..aM; b2..bM] of body i);
-    ``type`` and ``parent`` are 1-based ids."""
+    ``coef`` is ``ncoef × N`` (column i = [a0; a2..aM; b2..bM] of body i),
+    kept in Fortran (column-major) order as Julia stores it, so that a body's
+    coefficients are contiguous; ``type`` and ``parent`` are 1-based ids."""
 
     x: np.ndarray
     y: np.ndarray
@@ -254,9 +255,9 @@ class Bodies:
         y = np.array(y, dtype=np.float64).ravel()
         θ = np.array(θ, dtype=np.float64).ravel()
         R0 = np.array(R0, dtype=np.float64).ravel()
-        coef = np.array(coef, dtype=np.float64)
+        coef = np.array(coef, dtype=np.float64, order="F")
         if coef.ndim == 1:
-            coef = coef.reshape(-1, 1)
+            coef = np.asfortranarray(coef.reshape(-1, 1))
         if not (len(y) == len(θ) == len(R0) == N and coef.shape[1] == N):
             raise DimensionMismatch("inconsistent body array lengths")
         typ = np.full(N, int(type), dtype=np.int32) if np.isscalar(type) else np.array(type, dtype=np.int32).ravel()
@@ -291,7 +292,7 @@ def vcat(*bs: Bodies) -> Bodies:
     cat = lambda f: np.concatenate([getattr(b, f) for b in bs])
     parent = np.concatenate([b.parent + np.int32(o) for b, o in zip(bs, offs)]).astype(np.int32)
     return Bodies(cat("x"), cat("y"), cat("θ"), cat("imgx").astype(np.int32), cat("imgy").astype(np.int32),
-                  np.hstack([b.coef for b in bs]), cat("R0"), cat("type").astype(np.int32), parent)
+                  np.asfortranarray(np.hstack([b.coef for b in bs])), cat("R0"), cat("type").astype(np.int32), parent)
 
 
 def _rng(rng, seed):
@@ -317,7 +318,7 @@ def hexagonal_monolayer(nx, ny, packing=0.95, R0=1.0, maxmode=6, rng=None):
     x = (2 * col + (row % 2)) * r
     y = math.sqrt(3) * r * row
     θ = 2 * math.pi * _rng(rng, 1).random(N)
-    coef = np.zeros((2 * maxmode - 1, N))
+    coef = np.zeros((2 * maxmode - 1, N), order="F")
     coef[0, :] = 1.0
     return Bodies.new(x, y, θ, coef, np.full(N, float(R0))), box
 
@@ -325,7 +326,7 @@ def hexagonal_monolayer(nx, ny, packing=0.95, R0=1.0, maxmode=6, rng=None):
 def with_nuclei(cells: Bodies, ratio=0.5, type=2, rng=None):
     """Append one round nucleus per body (src/initial.jl:41-53)."""
     N = cells.n
-    coef = np.zeros_like(cells.coef)
+    coef = np.zeros(cells.coef.shape, order="F")
     coef[0, :] = 1.0
     θ = 2 * math.pi * _rng(rng, 2).random(N)
     nuclei = Bodies.new(cells.x.copy(), cells.y.copy(), θ, coef, ratio * cells.R0, type=type)

@@ -27,8 +27,8 @@ _POOL_SIG = {
     "pool_destroy": [C.c_void_p],
     "pool_add": [C.c_void_p, C.POINTER(abi.FccParams), C.POINTER(abi.FccBodiesHost), C.c_int64,
                  C.POINTER(C.c_int32)],
-    "pool_add_at": [C.c_void_p, C.POINTER(abi.FccParams), C.POINTER(abi.FccBodiesHost), C.c_int64, C.c_int64,
-                    C.POINTER(C.c_int32)],
+    "pool_add_at": [C.c_void_p, C.POINTER(abi.FccParams), C.POINTER(abi.FccBodiesHost), C.c_int64, C.c_double,
+                    C.c_int64, C.POINTER(C.c_int32)],
     "pool_remove": [C.c_void_p, C.c_int32],
     "pool_run": [C.c_void_p, C.c_int64],
     "pool_slot": [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
@@ -134,18 +134,22 @@ class Pool:
 
     # ------------------------------------------------------------ slots
     def add(self, bodies: Bodies, box, types, energies=(), bonds=(), dt=0.005, seed=1, skin=0.3, horizon=0,
-            nl_capacity=32, clock=0) -> int:
+            nl_capacity=32, clock=0, t=None) -> int:
         """Admit a simulation (the arguments of ``Simulation``); raises PoolFull
         when it does not fit now.  ``clock`` > 0 resumes a checkpoint (the
-        state and clock ``state`` returned): it holds at clock ``horizon``."""
+        state, clock and time ``state`` returned): it holds at clock
+        ``horizon``; without ``t`` its time restarts at clock * dt."""
         params = abi.ParamsBuffer(box, types, energies, bonds, dt, self.nθ, self.T, seed, skin, nl_capacity)
-        buf = abi.BodiesBuffer.from_bodies(bodies)
+        host = abi.direct_host(bodies)
+        if host is None:
+            buf = abi.BodiesBuffer.from_bodies(bodies)
+            host = buf.s
         slot = C.c_int32()
         if clock:
-            self._call("pool_add_at", self._h, C.byref(params.p), C.byref(buf.s), int(clock), int(horizon),
-                       C.byref(slot))
+            self._call("pool_add_at", self._h, C.byref(params.p), C.byref(host), int(clock),
+                       -1.0 if t is None else float(t), int(horizon), C.byref(slot))
         else:
-            self._call("pool_add", self._h, C.byref(params.p), C.byref(buf.s), int(horizon), C.byref(slot))
+            self._call("pool_add", self._h, C.byref(params.p), C.byref(host), int(horizon), C.byref(slot))
         self._slots[slot.value] = (bodies.n, bodies.ncoef, np.array(bodies.type, dtype=np.int32), box)
         return slot.value
 
@@ -199,7 +203,8 @@ class Pool:
         buf = abi.BodiesBuffer(n, ncoef)
         clk, t, stp = C.c_int64(), C.c_double(), C.c_int64()
         self._call("pool_get_state", self._h, int(slot), C.byref(buf.s), C.byref(clk), C.byref(t), C.byref(stp))
-        return buf.to_bodies(), clk.value, t.value, stp.value
+        b = Bodies(buf.x, buf.y, buf.theta, buf.imgx, buf.imgy, buf.coefT.T, buf.R0, buf.type, buf.parent)
+        return b, clk.value, t.value, stp.value
 
     def bodies(self, slot: int) -> Bodies:
         return self.state(slot)[0]

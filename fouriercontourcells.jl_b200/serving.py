@@ -98,11 +98,13 @@ class Server:
         self._cancel = set()
         self._cancel_lock = threading.Lock()
 
-    def cancel(self, request_id: int):
+    def cancel(self, request):
         """Withdraw a request: at the next chunk boundary it leaves the queue
-        or the pool (safe to call from the result callback or another thread)."""
+        or the pool (safe to call from the result callback or another thread).
+        ``request`` is the ``Request`` itself, or an id, which withdraws every
+        request of the stream that carries that id (ids need not be unique)."""
         with self._cancel_lock:
-            self._cancel.add(request_id)
+            self._cancel.add(("obj", id(request)) if isinstance(request, Request) else ("id", int(request)))
 
     def _take_cancelled(self):
         with self._cancel_lock:
@@ -123,7 +125,7 @@ class Server:
         waiting = deque()
         active = {}  # slot -> (request, first admitted)
         results = []
-        resume = {}  # id(request) -> (state, clock) of an evicted request
+        resume = {}  # id(request) -> (state, clock, time) of an evicted request
         first = {}   # id(request) -> first admission time (keyed by object: ids need not be unique)
         t0 = self.clock()
         now = lambda: self.clock() - t0
@@ -134,9 +136,9 @@ class Server:
         steps_now = {}  # slot -> steps done, read once per admission pass (steps change only in runs)
 
         def admit(q):
-            b, c = resume.get(id(q), (q.bodies, 0))
+            b, c, tq = resume.get(id(q), (q.bodies, 0, 0.0))
             if c:
-                slot = self.pool.try_add(b, q.box, horizon=q.horizon, clock=c, **q.kw)
+                slot = self.pool.try_add(b, q.box, horizon=q.horizon, clock=c, t=tq, **q.kw)
             else:
                 slot = self.pool.try_add(b, q.box, horizon=q.horizon, **q.kw)
             if slot is not None:
@@ -147,15 +149,16 @@ class Server:
             return slot
 
         while pending or waiting or active:
-            ids = self._take_cancelled()
-            if ids:
-                for q in [q for q in list(waiting) + list(pending) if q.id in ids]:  # not running
-                    b, c = resume.pop(id(q), (None, 0))
+            marks = self._take_cancelled()
+            if marks:
+                hit = lambda q: ("obj", id(q)) in marks or ("id", q.id) in marks
+                for q in [q for q in list(waiting) + list(pending) if hit(q)]:  # not running
+                    b, c, _ = resume.pop(id(q), (None, 0, 0.0))
                     results.append(Result(q.id, q.bodies.n, q.horizon, q.arrival, first.get(id(q), float("nan")),
                                           now(), b, cancelled=True, steps=c))
-                waiting = deque(q for q in waiting if q.id not in ids)
-                pending = deque(q for q in pending if q.id not in ids)
-                for s in [s for s, (r, _) in active.items() if r.id in ids]:
+                waiting = deque(q for q in waiting if not hit(q))
+                pending = deque(q for q in pending if not hit(q))
+                for s in [s for s, (r, _) in active.items() if hit(r)]:
                     r, adm = active.pop(s)
                     steps = self.pool.slot(s)[1]
                     b = self.pool.bodies(s)
@@ -183,7 +186,8 @@ class Server:
                         if work_left[s] < self.evict_ratio * left_of(r):
                             break
                         v, _ = active.pop(s)
-                        resume[id(v)] = (self.pool.bodies(s), steps_now.pop(s))
+                        b, _, tv, _ = self.pool.state(s)
+                        resume[id(v)] = (b, steps_now.pop(s), tv)
                         self.pool.remove(s)
                         self.evictions += 1
                         evicted.append(v)

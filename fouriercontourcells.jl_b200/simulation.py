@@ -16,12 +16,13 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 from collections import namedtuple
 
 import numpy as np
 
 from . import abi
-from .model import ArgumentError, Bodies, DeviceError
+from .model import ArgumentError, Bodies, DeviceError, DimensionMismatch
 
 Gradients = namedtuple("Gradients", "GR GD GDD P gx gy gθ glab gcoef Ebody")
 Geometry = namedtuple("Geometry", "lab labR0 R dR ddR rmax")
@@ -50,8 +51,34 @@ def native_library():
         lib.fcc_health.restype = C.c_int32
         lib.fcc_barrier_selftest.argtypes = [C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
         lib.fcc_barrier_selftest.restype = C.c_int32
+        lib.fcc_host_alloc.argtypes = [C.c_int64, C.POINTER(C.c_void_p)]
+        lib.fcc_host_alloc.restype = C.c_int32
+        lib.fcc_host_free.argtypes = [C.c_void_p]
+        lib.fcc_host_free.restype = C.c_int32
         _LIB = lib
     return _LIB
+
+
+def pinned_bodies(n: int, ncoef: int) -> Bodies:
+    """A ``Bodies`` of n bodies in page-locked host memory (``fcc_host_alloc``),
+    laid out as the C ABI reads and writes it, so ``set_state`` and
+    ``get_state(out=...)`` move it to and from the device by DMA with no host
+    copy.  The memory is released when the last of its arrays is collected."""
+    lib = native_library()
+    nbytes = abi.bodies_bytes(n, ncoef)
+    ptr = C.c_void_p()
+    abi.check(lib.fcc_host_alloc(nbytes, C.byref(ptr)), lib._lasterr)
+    block = np.frombuffer((C.c_uint8 * nbytes).from_address(ptr.value), dtype=np.uint8)
+    weakref.finalize(block, lib.fcc_host_free, ptr.value)
+    return abi.bodies_over(block, n, ncoef)
+
+
+def pinned_copy(bodies: Bodies) -> Bodies:
+    """``bodies`` copied into page-locked host memory (``pinned_bodies``)."""
+    out = pinned_bodies(bodies.n, bodies.ncoef)
+    for f in ("x", "y", "θ", "imgx", "imgy", "coef", "R0", "type", "parent"):
+        getattr(out, f)[...] = getattr(bodies, f)
+    return out
 
 
 class NativeSimulation:
@@ -70,9 +97,9 @@ class NativeSimulation:
         self._lib = self._library()
         self._fn = lambda name: getattr(self._lib, self._pfx + name)
         self._params = abi.ParamsBuffer(box, types, energies, bonds, dt, nθ, T, seed, skin, nl_capacity)
-        buf = abi.BodiesBuffer.from_bodies(bodies)
+        self._buf = None  # host arrays in the ABI's layout, reused for inputs that are not
         h = C.c_void_p()
-        self._call("create", C.byref(self._params.p), C.byref(buf.s), C.byref(h))
+        self._call("create", C.byref(self._params.p), C.byref(self._host_in(bodies)), C.byref(h))
         self._h = h
         self.N = bodies.n
         self.ncoef = bodies.ncoef
@@ -122,33 +149,62 @@ class NativeSimulation:
         return self.compute_gradients()
 
     # ---------------------------------------------------------------- state
-    def _state(self):
-        buf = abi.BodiesBuffer(self.N, self.ncoef)
+    def _host_in(self, bodies: Bodies):
+        """An ``fcc_bodies_host`` over `bodies` itself when its arrays are in
+        the ABI's layout, else over a copy in a buffer this object keeps."""
+        h = abi.direct_host(bodies)
+        if h is not None:
+            return h
+        if self._buf is None or self._buf.n != bodies.n or self._buf.ncoef != bodies.ncoef:
+            self._buf = abi.BodiesBuffer(bodies.n, bodies.ncoef)
+        self._buf.fill(bodies)
+        return self._buf.s
+
+    def _counters(self):
         clock, t, stp = C.c_int64(), C.c_double(), C.c_int64()
-        self._call("get_state", self._h, C.byref(buf.s), C.byref(clock), C.byref(t), C.byref(stp))
-        return buf, clock.value, t.value, stp.value
+        self._call("get_state", self._h, None, C.byref(clock), C.byref(t), C.byref(stp))
+        return clock.value, t.value, stp.value
+
+    def get_state(self, out: Bodies = None) -> Bodies:
+        """The body state (the fields of sim.bodies) copied to the host: into
+        `out` when given (its arrays are written in place, which takes one
+        device-to-host copy per array when they are in the ABI's layout, a DMA
+        when `out` is ``pinned_bodies``), else into new arrays."""
+        if out is not None:
+            h = abi.direct_host(out, writable=True)
+            if h is None or out.n != self.N or out.ncoef != self.ncoef:
+                raise ArgumentError("get_state(out=...) needs writable arrays of this simulation's size in the "
+                                    "ABI's layout (contiguous vectors, coef in Fortran order): see pinned_bodies")
+            self._call("get_state", self._h, C.byref(h), None, None, None)
+            return out
+        buf = abi.BodiesBuffer(self.N, self.ncoef)
+        self._call("get_state", self._h, C.byref(buf.s), None, None, None)
+        return Bodies(buf.x, buf.y, buf.theta, buf.imgx, buf.imgy, buf.coefT.T, buf.R0, buf.type, buf.parent)
 
     @property
     def bodies(self) -> Bodies:
         """Host copy of sim.bodies."""
-        return self._state()[0].to_bodies()
+        return self.get_state()
 
     @property
     def clock(self) -> int:
-        return self._state()[1]
+        return self._counters()[0]
 
     @property
     def t(self) -> float:
-        return self._state()[2]
+        return self._counters()[1]
 
     @property
     def nsteps(self) -> int:
         """sim.step of the reference (steps taken)."""
-        return self._state()[3]
+        return self._counters()[2]
 
     def set_state(self, bodies: Bodies, clock: int = -1):
-        buf = abi.BodiesBuffer.from_bodies(bodies)
-        self._call("set_state", self._h, C.byref(buf.s), int(clock))
+        """Overwrite the body state and the clock (``fcc_set_state``); R0,
+        type and parent must be the created ones."""
+        if bodies.n != self.N or bodies.ncoef != self.ncoef:
+            raise DimensionMismatch("state buffers do not match the simulation")
+        self._call("set_state", self._h, C.byref(self._host_in(bodies)), int(clock))
         return self
 
     @property

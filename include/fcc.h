@@ -177,8 +177,19 @@ fcc_status fcc_get_state(fcc_sim* sim, fcc_bodies_host* out, int64_t* clock, dou
 /* Overwrite the body state (x, y, theta, imgx, imgy, coef; R0, type and parent
  * must match the created ones) and the clock; then enforce_shape!,
  * update_geometry! and an invalidated neighbour list, like the tests' refresh!
- * (test/runtests.jl:9-15). `clock < 0` keeps the clock. */
+ * (test/runtests.jl:9-15). `clock < 0` keeps the clock.  The arrays are read
+ * once, as they are; the call returns when they are no longer needed. */
 fcc_status fcc_set_state(fcc_sim* sim, const fcc_bodies_host* in, int64_t clock);
+
+/* Page-locked host memory for the arrays of fcc_bodies_host (no counterpart
+ * in the reference, whose host arrays are Julia Arrays and whose state stays
+ * in CuArrays).  fcc_set_state and fcc_get_state copy the caller's arrays to
+ * and from the device as they are, converting on the device; from memory
+ * allocated here those copies are direct DMA transfers, from ordinary
+ * (pageable) memory the CUDA driver stages them through its own buffers.
+ * A maintainer binding Julia would instead pin with CUDA.Mem.pin. */
+fcc_status fcc_host_alloc(int64_t bytes, void** out);
+fcc_status fcc_host_free(void* ptr);
 
 /* sim.dt = dt (test/test_cuda.jl:156-162). */
 fcc_status fcc_set_dt(fcc_sim* sim, double dt);
@@ -301,14 +312,15 @@ fcc_status fcc_pool_destroy(fcc_pool* pool);
  * FCC_ERR_FULL: no free slot, bodies or cells now (nothing changed). */
 fcc_status fcc_pool_add(fcc_pool* pool, const fcc_params* params, const fcc_bodies_host* bodies, int64_t horizon,
                         int32_t* slot);
-/* Admit a simulation resumed from a checkpoint: `bodies` and `clock` as
+/* Admit a simulation resumed from a checkpoint: `bodies`, `clock` and `t` as
  * fcc_get_state / fcc_pool_get_state returned them (the clock is the Philox
- * draw index, src/random.jl:103); it holds when its clock reaches `horizon`,
- * and its steps done count from `clock`.  The state is loaded with the same
- * arithmetic as fcc_set_state (no counterpart in the reference: the serving
- * loop evicts and re-admits with it). */
+ * draw index, src/random.jl:103; t is sim.t, which differs from clock * dt
+ * once dt has changed); it holds when its clock reaches `horizon`, and its
+ * steps done count from `clock`.  t < 0 takes clock * dt.  The state is
+ * loaded with the same arithmetic as fcc_set_state (no counterpart in the
+ * reference: the serving loop evicts and re-admits with it). */
 fcc_status fcc_pool_add_at(fcc_pool* pool, const fcc_params* params, const fcc_bodies_host* bodies, int64_t clock,
-                           int64_t horizon, int32_t* slot);
+                           double t, int64_t horizon, int32_t* slot);
 /* Retire a simulation; its room is reclaimed before the next run or add. */
 fcc_status fcc_pool_remove(fcc_pool* pool, int32_t slot);
 

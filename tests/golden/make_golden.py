@@ -1,8 +1,8 @@
 """Generate the golden fixtures of tests/golden/ from the reference's own tests.
 
-Run in a checkout that has the reference mounted (default /root/reference):
+Run with the path of a checkout of the reference:
 
-    python tests/golden/make_golden.py [REFERENCE_DIR]
+    python tests/golden/make_golden.py REFERENCE_DIR
 
 Writes
   - reference_N64.npz: the regression fixture test/data/reference_N64.txt
@@ -64,4 +64,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_DIR")
+    main(sys.argv[1])

@@ -38,8 +38,9 @@ def test_oracle_exports_mirror():
     lib = oracle.library()
     for n in declared_functions():
         if n in ("fcc_run", "fcc_last_timing", "fcc_version", "fcc_build_neighbors_noalloc", "fcc_health",
-                 "fcc_barrier_selftest") or n.startswith("fcc_pool_"):
-            continue  # device-only entry points (launch timing, caller device arrays, device health, packed pools)
+                 "fcc_barrier_selftest", "fcc_host_alloc", "fcc_host_free") or n.startswith("fcc_pool_"):
+            continue  # device-only entry points (launch timing, caller device arrays, device health, packed
+            # pools, page-locked host memory)
         assert hasattr(lib, "fcco_" + n[4:]), n
 
 

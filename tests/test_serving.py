@@ -66,6 +66,10 @@ class FakePool:
     def bodies(self, s):
         return self.sims[s]["bodies"]
 
+    def state(self, s):
+        x = self.sims[s]
+        return x["bodies"], x["steps"], 0.005 * x["steps"], x["steps"]
+
     def shape_index(self, s):
         return np.full(self.sims[s]["n"], 3.6)
 
@@ -261,3 +265,44 @@ def test_requests_without_distinct_ids_keep_their_own_admission_times():
     adm = sorted(r.admitted for r in res)
     assert len(res) == 3 and adm[0] < adm[1] < adm[2]
     assert all(r.admitted < r.finished for r in res)
+
+
+def test_cancel_by_request_object_leaves_equal_ids_alone():
+    """Requests that share an id (the default 0) are cancelled one by one by
+    passing the Request itself; cancelling by id withdraws all that carry it."""
+    clk = FakeClock()
+    pool = FakePool(clk, max_bodies=256, max_sims=1)
+    reqs = [fcc.Request(q.bodies, q.box, q.kw, q.horizon, q.arrival) for q in
+            (req(0, 4, 4, 100, 0.0), req(1, 4, 4, 100, 0.0), req(2, 4, 4, 100, 0.0))]
+    srv = fcc.Server(pool, chunk=64, min_chunk=1, clock=clk, sleep=clk.sleep)
+    srv.cancel(reqs[1])  # still waiting when the loop starts: never admitted
+    res = srv.serve(reqs)
+    by_seed = {r.bodies is None: r for r in res}
+    assert len(res) == 3 and sum(r.cancelled for r in res) == 1
+    assert by_seed[True].cancelled and by_seed[True].steps == 0
+    assert sum(1 for e in pool.log if e[0] == "add") == 2
+    srv = fcc.Server(fcc_pool := FakePool(clk, max_bodies=256, max_sims=1), chunk=64, min_chunk=1, clock=clk,
+                     sleep=clk.sleep)
+    srv.cancel(0)
+    res = srv.serve(reqs)
+    assert len(res) == 3 and all(r.cancelled for r in res)
+    assert not any(e[0] == "add" for e in fcc_pool.log)
+
+
+def test_evicted_request_resumes_with_its_own_time():
+    """Eviction saves the state, clock and time the pool reports and
+    re-admits with all three (a resumed time is not recomputed as clock * dt)."""
+    clk = FakeClock()
+    pool = FakePool(clk, max_bodies=128, max_sims=8)
+    seen = []
+    orig = pool.try_add
+
+    def try_add(bodies, box, horizon, clock=0, **kw):
+        seen.append((clock, kw.get("t")))
+        return orig(bodies, box, horizon, clock=clock, **kw)
+
+    pool.try_add = try_add
+    reqs = [req(0, 8, 12, 4000, 0.0), req(1, 8, 8, 200, 0.001)]
+    fcc.Server(pool, chunk=128, min_chunk=1, clock=clk, sleep=clk.sleep, policy="evict").serve(reqs)
+    resumed = [(c, t) for c, t in seen if c]
+    assert resumed and all(t == pytest.approx(0.005 * c) for c, t in resumed)
