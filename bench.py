@@ -339,6 +339,32 @@ def make_request(fcc, sp):
     return fcc.Request(bodies, box, kw, sp["horizon"], sp["arrival"], sp["id"])
 
 
+AUDIT_STEPS = 10
+
+
+def trajectory_audit(fcc, oracle, r, steps=AUDIT_STEPS):
+    """The first `steps` steps of request r in FP32 on the GPU (its solo run,
+    which the served result equals bit for bit) against the FP64 oracle from
+    the same FP32-representable initial state and Philox stream.  Stated
+    tolerance: 95% of the bodies within 4 FP32 ulps of their coordinates in
+    position and 1e-6 in every shape coefficient, and all within 2e-3 (a node
+    at an Overlap near-tie may flip its Heaviside contact in FP32)."""
+    b = r.bodies.copy()
+    for f in ("x", "y", "θ", "coef", "R0"):
+        setattr(b, f, np.asfortranarray(np.asarray(getattr(b, f), np.float32).astype(np.float64)))
+    g = fcc.Simulation(b, r.box, T=np.float32, **r.kw).run(steps)
+    o = oracle.OracleSimulation(b, r.box, T=np.float64, **r.kw).step(steps)
+    bg, bo = g.bodies, o.bodies
+    g.close()
+    Lx, Ly = r.box.Lx, r.box.Ly
+    dr = np.hypot(bg.x + bg.imgx * Lx - bo.x - bo.imgx * Lx, bg.y + bg.imgy * Ly - bo.y - bo.imgy * Ly)
+    dc = np.abs(bg.coef - bo.coef).max(axis=0)
+    ulp = np.spacing(np.maximum(np.abs(bo.x), np.abs(bo.y)).astype(np.float32)).astype(np.float64)
+    within = float(np.mean((dr < 4 * ulp) & (dc < 1e-6)))
+    return {"n": b.n, "max_dr": float(dr.max()), "max_dcoef": float(dc.max()), "frac_within": within,
+            "pass": bool(within >= 0.95 and dr.max() < 2e-3 and dc.max() < 2e-3)}
+
+
 def serving_leg(fcc, oracle, work=1.5e10, pool_bodies=1 << 18, policy="fifo"):
     """The first requests of the serving stream (up to `work` body-steps),
     served by continuous batching on one pool sized from an HBM budget, then
@@ -376,9 +402,15 @@ def serving_leg(fcc, oracle, work=1.5e10, pool_bodies=1 << 18, policy="fifo"):
     plain_span = max(a + l for a, l in zip((r.arrival for r in reqs), lat)) - min(r.arrival for r in reqs)
     plain = {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
              "body_steps_per_s": served["body_steps"] / plain_span}
-    # 1% audited sample (at least one request): force error of the served result
-    audit = [r for r in reqs if r.id % 100 == 0] or reqs[:1]
-    errs = {r.id: force_error(fcc, oracle, by_id[r.id].bodies, r.box, r.kw)["max_rel"] for r in audit}
+    # audited requests: at least 20 (or all), spread over the sample; each
+    # served result equals its solo run bit for bit (checked above for every
+    # request), so the audit checks that solo path against the FP64 oracle:
+    # the first steps of its trajectory, and the forces of its final state
+    audit = reqs[::max(1, len(reqs) // 20)] if len(reqs) >= 20 else list(reqs)
+    errs, traj = {}, {}
+    for r in audit:
+        errs[r.id] = force_error(fcc, oracle, by_id[r.id].bodies, r.box, r.kw)["max_rel"]
+        traj[r.id] = trajectory_audit(fcc, oracle, r)
     u = pool.usage()
     pool.close()
     return {"workload": SERVE_WORKLOAD,
@@ -389,7 +421,16 @@ def serving_leg(fcc, oracle, work=1.5e10, pool_bodies=1 << 18, policy="fifo"):
             "served_over_plain": served["body_steps_per_s"] / plain["body_steps_per_s"],
             "chunks": srv.chunks, "device_busy_fraction": srv.device_ms * 1e-3 / max(served["makespan_s"], 1e-9),
             "bitwise_equal_to_alone": f"{equal}/{len(reqs)}",
-            "audit_force_error_vs_fp64": errs}
+            "audited": len(audit),
+            "audit_force_error_vs_fp64": errs,
+            "audit_trajectory_vs_fp64": {
+                "steps": AUDIT_STEPS, "passed": f"{sum(t['pass'] for t in traj.values())}/{len(traj)}",
+                "worst_max_dr": max(t["max_dr"] for t in traj.values()),
+                "worst_max_dcoef": max(t["max_dcoef"] for t in traj.values()),
+                "min_frac_within": min(t["frac_within"] for t in traj.values()),
+                "tolerance": "95% of bodies within 4 FP32 ulps of their coordinates and 1e-6 in every shape "
+                             "coefficient, all within 2e-3 (an Overlap near-tie may flip in FP32)",
+                "per_request": traj}}
 
 
 # ------------------------------------------------------------------ arms

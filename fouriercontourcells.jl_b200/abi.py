@@ -37,7 +37,8 @@ class FccTerm(C.Structure):
 
 class FccBodyType(C.Structure):
     _fields_ = [("v0", C.c_double), ("Dr", C.c_double), ("Dt", C.c_double), ("mu_r", C.c_double),
-                ("mu_theta", C.c_double), ("mu_ab", C.c_double), ("parent_drag", C.c_int32)]
+                ("mu_theta", C.c_double), ("mu_ab", C.c_double), ("parent_drag", C.c_int32),
+                ("maxmode", C.c_int32)]
 
 
 class FccParams(C.Structure):
@@ -149,7 +150,8 @@ class ParamsBuffer:
             raise ArgumentError("at most 16 energy terms")
         self.types = (FccBodyType * len(types))()
         for q, t in enumerate(types):
-            self.types[q] = FccBodyType(t.v0, t.Dr, t.Dt, t.mu_r, t.mu_theta, t.mu_ab, 1 if t.parent_drag else 0)
+            self.types[q] = FccBodyType(t.v0, t.Dr, t.Dt, t.mu_r, t.mu_theta, t.mu_ab, 1 if t.parent_drag else 0,
+                                        int(t.maxmode))
         self.terms = (FccTerm * max(1, len(energies)))()
         for q, e in enumerate(energies):
             self.terms[q] = _term_struct(e)

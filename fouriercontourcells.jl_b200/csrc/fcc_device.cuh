@@ -68,6 +68,7 @@ struct SimDesc {
     T v0[MT], Dr[MT], Dt[MT], mur[MT], muth[MT], muab[MT];
     T sigr[MT], sigt[MT];  // sqrt(2 Dr dt), sqrt(2 Dt dt) in T (noise amplitudes; set with dt)
     int parent_drag[MT];
+    int kmax[MT];  // shape modes a type may carry (modes m >= kmax stay zero), <= K
     int bt_kind[MTERM];
     uint32_t bt_mask[MTERM];
     T bt_a[MTERM], bt_b[MTERM];  // Tension: a = eta; PerimeterElasticity: a = lambda, b = p0*sqrt(pi)

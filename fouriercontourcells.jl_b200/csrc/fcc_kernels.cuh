@@ -783,6 +783,7 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
     const T h0 = ga0 / (T(2) * a0);  // dE/da0 * da0/da_n = -h0 a_n (area constraint)
     const T dtmu = dt * P.muab[ti];
     const int K = P.K;
+    const int Kt = min(K, P.kmax[ti]);  // modes of this type; the rest stay zero
     T an[MPL], bn[MPL];
     double sp = 0.0;
 #pragma unroll
@@ -790,7 +791,7 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
         const int m = l + u * L;
         an[u] = T(0);
         bn[u] = T(0);
-        if (m < K) {
+        if (m < Kt) {
             T ga = gl[1], gb = gl[1 + KM];
 #pragma unroll
             for (int mm = 1; mm < KM; ++mm)
@@ -1742,25 +1743,28 @@ __global__ void k_finish_rebuild(DevPtrs<T> d) {
 // Bodies g0 .. g0+n-1; the inputs are indexed from i = 0 and are the caller's
 // host values as they crossed the ABI (double), in the reference's
 // coefficient layout: in_nc values per body, [a0; a_2..a_{in_K+1};
-// b_2..b_{in_K+1}] (src/basis.jl:10-14).  Each value is rounded to T here,
-// exactly as a host-side conversion would round it.
+// b_2..b_{in_K+1}] (src/basis.jl:10-14), and the record words w = (parent <<
+// 3) | type (0-based).  Each value is rounded to T here, exactly as a
+// host-side conversion would round it.
 template <class T>
 __global__ void k_init(DevPtrs<T> d, int par, int g0, int n, const double* __restrict__ x,
                        const double* __restrict__ y, const double* __restrict__ th_in,
-                       const double* __restrict__ coef_in, int in_nc, int in_K) {
+                       const double* __restrict__ coef_in, int in_nc, int in_K, const int* __restrict__ w) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int g = g0 + i;
     const int s = d.sim_of[g];
     const SimDesc<T>& P = d.sims[s];
     const int K = P.K;
+    const int wi = w[i];
+    const int kt = min(in_K, P.kmax[wi & 7]);  // modes above the body type's maxmode enter as zero
     T c[NCM];
     const double* ci = coef_in + (size_t)i * in_nc;
     c[0] = T(ci[0]);
 #pragma unroll
     for (int m = 0; m < KM; ++m) {
-        c[1 + m] = m < in_K ? T(ci[1 + m]) : T(0);
-        c[1 + KM + m] = m < in_K ? T(ci[1 + in_K + m]) : T(0);
+        c[1 + m] = m < kt ? T(ci[1 + m]) : T(0);
+        c[1 + KM + m] = m < kt ? T(ci[1 + in_K + m]) : T(0);
     }
     const T th_i = T(th_in[i]);
     // enforce_shape! and the lab frame with the arithmetic of the update's
@@ -1833,19 +1837,12 @@ __global__ void k_init(DevPtrs<T> d, int par, int g0, int n, const double* __res
     rn[R_X] = T(x[i]);
     rn[R_Y] = T(y[i]);
     rn[R_RMAX] = r0 * bound;
-    rn[R_A0] = r0 * c[0];  // R_W (parent, type) is written by k_set_w
+    rn[R_A0] = r0 * c[0];
+    T* tag = nullptr;
+    rn[R_W] = pack_w(wi, tag);  // (parent, type)
     rn[R_TH] = th_i;
 #pragma unroll
     for (int r = 0; r < NCM; ++r) d.coef[(size_t)g * NCM + r] = c[r];
-}
-
-// w field (parent, type) of the current record
-template <class T>
-__global__ void k_set_w(DevPtrs<T> d, int par, int g0, int n, const int* __restrict__ w) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    T* tag = nullptr;
-    rec_cur_mut(d, par)[(size_t)(g0 + i) * RECW + R_W] = pack_w(w[i], tag);
 }
 
 // get_state on the device: x, y, theta of the current record and the

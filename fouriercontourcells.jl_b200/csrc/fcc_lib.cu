@@ -213,15 +213,37 @@ void set_noise_amplitudes(SimDesc<T>& s) {
     }
 }
 
+// Cell grid of CellList(box, cutoff, n) (src/neighbors.jl:27-45): floor(L /
+// cutoff) cells per side, collapsed to 1 below 3.  The box sides and the
+// cutoff must be finite and positive (the reference's floor(Int, L/cutoff)
+// throws otherwise), and the side counts are formed in 64 bits, each capped,
+// before anything narrows them.
+fcc_status cell_grid_dims(double Lx, double Ly, double cutoff, int64_t* ncx, int64_t* ncy) {
+    if (!(std::isfinite(cutoff) && cutoff > 0))
+        return fail(FCC_ERR_ARGUMENT, "cutoff must be a finite positive number");
+    if (!(std::isfinite(Lx) && Lx > 0 && std::isfinite(Ly) && Ly > 0))
+        return fail(FCC_ERR_ARGUMENT, "box sides must be finite positive numbers");
+    auto side = [&](double L, int64_t* out) -> fcc_status {
+        const double m = std::floor(L / cutoff);
+        if (!(m < (double)(1 << 28))) return fail(FCC_ERR_UNSUPPORTED, "cell grid too large");
+        *out = m >= 3 ? (int64_t)m : 1;
+        return FCC_OK;
+    };
+    FCC_TRY(side(Lx, ncx));
+    return side(Ly, ncy);
+}
+
 template <class T>
 fcc_status make_spec(const fcc_params* p, const fcc_bodies_host* b, SimSpec<T>& sp) {
     // validation in the order of src/simulation.jl:66-105
     if (!p || !b) return fail(FCC_ERR_ARGUMENT, "null argument");
     if (p->ntypes < 1 || p->ntypes > FCC_MAX_TYPES || !p->types)
         return fail(FCC_ERR_ARGUMENT, "types must hold 1..8 BodyType entries");
-    for (int t = 0; t < p->ntypes; ++t)
+    for (int t = 0; t < p->ntypes; ++t) {
         if (p->types[t].parent_drag != 0 && p->types[t].parent_drag != 1)
             return fail(FCC_ERR_ARGUMENT, "drag must be :substrate or :parent");
+        if (p->types[t].maxmode < 0) return fail(FCC_ERR_ARGUMENT, "a body type's maxmode must be >= 0");
+    }
     if (p->nterms < 0 || p->nterms > FCC_MAX_TERMS || (p->nterms > 0 && !p->terms))
         return fail(FCC_ERR_ARGUMENT, "energy terms must be BodyTerms, ContactTerms or BondTerms");
     for (int q = 0; q < p->nterms; ++q) {
@@ -269,6 +291,9 @@ fcc_status make_spec(const fcc_params* p, const fcc_bodies_host* b, SimSpec<T>& 
     nc = 2 * K + 1;
     if (b->ncoef != nc) return fail(FCC_ERR_DIMENSION, "coefficient rows must be odd: [a₀; aₙ; bₙ]");
     if (K > KM) return fail(FCC_ERR_UNSUPPORTED, "the kernels support maxmode ≤ 10");
+    for (int t = 0; t < p->ntypes; ++t)
+        if (p->types[t].maxmode > K + 1)
+            return fail(FCC_ERR_ARGUMENT, "a body type's maxmode exceeds the simulation's (" + std::to_string(K + 1) + ")");
     if (!(p->skin >= 0)) return fail(FCC_ERR_ARGUMENT, "skin must be non-negative");
 
     // simulation descriptor (convert_precision: every parameter to T)
@@ -296,13 +321,13 @@ fcc_status make_spec(const fcc_params* p, const fcc_bodies_host* b, SimSpec<T>& 
         maxR0 = std::max(maxR0, (double)R0_h[i]);
     }
     const double cutoff = 2 * maxR0 * (1 + SHAPE_BOUND) + 0.0 + p->skin;  // src/simulation.jl:90
-    auto ncells = [&](T L) {
-        int64_t n = (int64_t)std::floor((double)L / cutoff);
-        return (int)(n >= 3 ? n : 1);
-    };
-    ncx = ncells(s.Lx);
-    ncy = ncells(s.Ly);
-    if ((int64_t)ncx * ncy > (1 << 28)) return fail(FCC_ERR_UNSUPPORTED, "cell grid too large");
+    {
+        int64_t gx = 0, gy = 0;
+        FCC_TRY(cell_grid_dims((double)s.Lx, (double)s.Ly, cutoff, &gx, &gy));
+        if (gx * gy > (1 << 28)) return fail(FCC_ERR_UNSUPPORTED, "cell grid too large");
+        ncx = (int)gx;
+        ncy = (int)gy;
+    }
     s.wx = s.Lx / (T)ncx;
     s.wy = s.Ly / (T)ncy;
     s.ncx = ncx;
@@ -326,6 +351,7 @@ fcc_status make_spec(const fcc_params* p, const fcc_bodies_host* b, SimSpec<T>& 
         s.muth[t] = (T)bt.mu_theta;
         s.muab[t] = (T)bt.mu_ab;
         s.parent_drag[t] = bt.parent_drag;
+        s.kmax[t] = bt.maxmode > 0 ? bt.maxmode - 1 : K;
     }
     set_noise_amplitudes(s);
     auto mask_of = [](const fcc_term& ft) {
@@ -778,9 +804,8 @@ struct Engine final : EngineBase {
         const DevPtrs<T> d = ptrs();
         if (N > 0) {
             const int grid = (int)((N + 255) / 256);
-            k_init<T><<<grid, 256, 0, stream>>>(d, par(), 0, (int)N, dx, dx + n, dx + 2 * n, dx + 3 * n, nc, K);
-            CUDA_TRY(cudaGetLastError());
-            k_set_w<T><<<grid, 256, 0, stream>>>(d, par(), 0, (int)N, w_dev.p);
+            k_init<T><<<grid, 256, 0, stream>>>(d, par(), 0, (int)N, dx, dx + n, dx + 2 * n, dx + 3 * n, nc, K,
+                                                w_dev.p);
             CUDA_TRY(cudaGetLastError());
         }
         // list invalid: the next step (or update_neighbors!) rebuilds
@@ -1215,12 +1240,10 @@ fcc_status build_neighbors_t(int64_t n, const double* x, const double* y, const 
     SimDesc<T> s{};
     s.Lx = (T)Lx;
     s.Ly = (T)Ly;
-    auto ncells = [&](T L) {
-        int64_t m = (int64_t)std::floor((double)L / cutoff);
-        return (int)(m >= 3 ? m : 1);
-    };
-    const int ncx = ncells(s.Lx), ncy = ncells(s.Ly);
-    if ((int64_t)ncx * ncy > (1 << 28)) return fail(FCC_ERR_UNSUPPORTED, "cell grid too large");
+    int64_t gx = 0, gy = 0;
+    FCC_TRY(cell_grid_dims((double)s.Lx, (double)s.Ly, cutoff, &gx, &gy));
+    if (gx * gy > (1 << 28)) return fail(FCC_ERR_UNSUPPORTED, "cell grid too large");
+    const int ncx = (int)gx, ncy = (int)gy;
     s.wx = s.Lx / (T)ncx;
     s.wy = s.Ly / (T)ncy;
     s.ncx = ncx;

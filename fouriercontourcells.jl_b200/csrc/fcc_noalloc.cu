@@ -1,9 +1,8 @@
 // fcc_noalloc.cu — neighbour build that allocates no device memory.
 //
-// Some callers cannot call cudaMalloc: code running inside a CUDA stream
-// capture or a device-memory pool they do not own, allocators that forbid
-// foreign allocations in a serving process, or embedders whose memory budget
-// is fixed up front.  fcc_build_neighbors_noalloc serves them: the caller
+// Some callers cannot call cudaMalloc: code running inside a device-memory
+// pool it does not own, allocators that forbid foreign allocations in a
+// serving process, or embedders whose memory budget is fixed up front.  fcc_build_neighbors_noalloc serves them: the caller
 // passes its input and output arrays already on the device, and every other
 // buffer the cell-list / neighbour-list kernels need lives in the static
 // device array below, which each GPU that loads this library holds until the
@@ -117,15 +116,13 @@ fcc_status build_neighbors_noalloc_t(int64_t n, const T* x, const T* y, const T*
     SimDesc<T> s{};
     s.Lx = (T)Lx;
     s.Ly = (T)Ly;
-    auto ncells = [&](T L) {
-        const int64_t m = (int64_t)std::floor((double)L / cutoff);
-        return (int)(m >= 3 ? m : 1);
-    };
-    const int ncx = ncells(s.Lx), ncy = ncells(s.Ly);
-    if ((int64_t)ncx * ncy > FCC_NOALLOC_MAX_CELLS)
-        return fail(FCC_ERR_ARGUMENT, "the cell grid (" + std::to_string((int64_t)ncx * ncy) +
+    int64_t gx = 0, gy = 0;
+    FCC_TRY(cell_grid_dims((double)s.Lx, (double)s.Ly, cutoff, &gx, &gy));
+    if (gx * gy > FCC_NOALLOC_MAX_CELLS)
+        return fail(FCC_ERR_ARGUMENT, "the cell grid (" + std::to_string(gx * gy) +
                                           " cells) exceeds FCC_NOALLOC_MAX_CELLS = " +
                                           std::to_string(FCC_NOALLOC_MAX_CELLS));
+    const int ncx = (int)gx, ncy = (int)gy;
     s.wx = s.Lx / (T)ncx;
     s.wy = s.Ly / (T)ncy;
     s.ncx = ncx;
@@ -185,6 +182,14 @@ extern "C" fcc_status fcc_build_neighbors_noalloc(int32_t precision, int64_t n, 
     if (n > FCC_NOALLOC_MAX_BODIES)
         return fail(FCC_ERR_ARGUMENT, "n = " + std::to_string(n) + " exceeds FCC_NOALLOC_MAX_BODIES = " +
                                           std::to_string(FCC_NOALLOC_MAX_BODIES));
+    {  // the grid first: a cutoff or box that is not finite and positive, or a grid beyond the scratch
+        int64_t gx = 0, gy = 0;
+        const fcc_status g = cell_grid_dims(Lx, Ly, cutoff, &gx, &gy);
+        if (g == FCC_ERR_UNSUPPORTED || (g == FCC_OK && gx * gy > FCC_NOALLOC_MAX_CELLS))
+            return fail(FCC_ERR_ARGUMENT, "the cell grid exceeds FCC_NOALLOC_MAX_CELLS = " +
+                                              std::to_string(FCC_NOALLOC_MAX_CELLS) + " cells");
+        if (g != FCC_OK) return g;
+    }
     if (n == 0) return FCC_OK;
     if (!x || !y || !rmax || !cellid || !perm || !start || !stop || !idx || !count)
         return fail(FCC_ERR_ARGUMENT, "null device array");

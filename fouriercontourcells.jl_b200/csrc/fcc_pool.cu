@@ -498,7 +498,7 @@ struct Pool final : PoolBase {
         return sync_stream();
     }
 
-    // enforce_shape! and lab frame of a slot's host state (k_init, k_set_w):
+    // enforce_shape! and lab frame of a slot's host state (k_init):
     // the caller's double arrays are copied as they are and converted on the
     // device
     fcc_status load_bodies(int s, const fcc_bodies_host* b) {
@@ -518,9 +518,7 @@ struct Pool final : PoolBase {
         const DevPtrs<T> d = ptrs();
         const int blocks = (int)((n + 255) / 256);
         k_init<T><<<blocks, 256, 0, stream>>>(d, par(), (int)S.off, (int)n, dx, dx + n, dx + 2 * n, dx + 3 * n, P.nc,
-                                              P.K);
-        CUDA_TRY(cudaGetLastError());
-        k_set_w<T><<<blocks, 256, 0, stream>>>(d, par(), (int)S.off, (int)n, st_w.p());
+                                              P.K, st_w.p());
         CUDA_TRY(cudaGetLastError());
         return sync_stream();
     }

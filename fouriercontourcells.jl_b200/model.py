@@ -46,7 +46,9 @@ class BodyType:
     """Dynamical parameters of one body type (src/bodies.jl:30-45).
 
     Accepts the reference's keyword names ``v0, Dr, Dt, μr, μθ, μab, drag``
-    (ASCII aliases ``mu_r, mu_theta, mu_ab``)."""
+    (ASCII aliases ``mu_r, mu_theta, mu_ab``).  ``maxmode`` (not in the
+    reference, whose types all share the simulation's modes) limits this
+    type's shape modes to n = 2..maxmode; 0 keeps every mode."""
 
     v0: float = 0.0
     Dr: float = 0.0
@@ -55,8 +57,10 @@ class BodyType:
     mu_theta: float = 1.0
     mu_ab: float = 0.1
     drag: str = "substrate"
+    maxmode: int = 0
 
-    def __init__(self, v0=0.0, Dr=0.0, Dt=0.0, mu_r=None, mu_theta=None, mu_ab=None, drag="substrate", **kw):
+    def __init__(self, v0=0.0, Dr=0.0, Dt=0.0, mu_r=None, mu_theta=None, mu_ab=None, drag="substrate", maxmode=0,
+                 **kw):
         μr = kw.pop("μr", None)
         μθ = kw.pop("μθ", None)
         μab = kw.pop("μab", None)
@@ -72,6 +76,9 @@ class BodyType:
         object.__setattr__(self, "mu_theta", float(mu_theta if mu_theta is not None else (μθ if μθ is not None else 1.0)))
         object.__setattr__(self, "mu_ab", float(mu_ab if mu_ab is not None else (μab if μab is not None else 0.1)))
         object.__setattr__(self, "drag", drag)
+        if int(maxmode) != maxmode or maxmode < 0:
+            raise ArgumentError(f"maxmode must be a non-negative integer, got {maxmode}")
+        object.__setattr__(self, "maxmode", int(maxmode))
 
     @property
     def parent_drag(self) -> bool:

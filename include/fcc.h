@@ -74,10 +74,15 @@ typedef struct {
 } fcc_term;
 
 /* BodyType(; v0, Dr, Dt, mu_r, mu_theta, mu_ab, drag) (src/bodies.jl:30-45);
- * parent_drag = 1 is drag = :parent. */
+ * parent_drag = 1 is drag = :parent.  maxmode limits the shape modes of this
+ * type's bodies to n = 2..maxmode (0: every mode of the simulation; 1: none,
+ * rigid circles): modes above it are zero on entry and stay zero.  No
+ * counterpart in the reference, where every type shares the simulation's
+ * ncoef (docs/nucleus.md:121-122); maxmode = 0 is the reference's behaviour. */
 typedef struct {
     double v0, Dr, Dt, mu_r, mu_theta, mu_ab;
     int32_t parent_drag;
+    int32_t maxmode;
 } fcc_body_type;
 
 /* Keyword arguments of Simulation(bodies, box; ...) (src/simulation.jl:66-68). */
@@ -229,20 +234,23 @@ fcc_status fcc_build_neighbors(int32_t precision, int64_t n, const double* x, co
 
 /* Neighbour build that allocates no device memory (no counterpart in the
  * reference, which allocates its lists itself).  For callers that cannot call
- * cudaMalloc — inside stream capture, under a memory pool or allocator they do
- * not own, or with a device-memory budget fixed up front — this does what
+ * cudaMalloc — code that runs inside a memory pool or allocator it does not
+ * own, or with a device-memory budget fixed up front — this does what
  * fcc_build_neighbors does, but on arrays already on the device: inputs x, y,
  * rmax (n values, float for precision 32, double for 64) and outputs cellid,
  * perm, count (n), start, stop (ncx*ncy) and idx (cap x n), in the same 1-based
  * layout.  All other scratch lives in one static device array of this
  * library, about 3.6 MB, which every GPU that loads the library holds until
  * the process exits; sizes beyond FCC_NOALLOC_MAX_BODIES bodies or
- * FCC_NOALLOC_MAX_CELLS grid cells return FCC_ERR_ARGUMENT.  Work is queued
- * on `stream` (a cudaStream_t; NULL: the default stream) and the call returns
+ * FCC_NOALLOC_MAX_CELLS grid cells, and a cutoff or box side that is not a
+ * finite positive number, return FCC_ERR_ARGUMENT.  Work is queued on
+ * `stream` (a cudaStream_t; NULL: the default stream) and the call returns
  * without synchronising.  The first call on a device looks up the scratch
- * array's device address (make that first call before any stream capture).
- * Every call reuses the same scratch, so calls that overlap on the GPU (other
- * streams, other threads) race: serialise them. */
+ * array's device address and keeps it for the process (make that first call
+ * before any stream capture; after cudaDeviceReset on that device the kept
+ * address is stale and later calls there are invalid).  Every call reuses the
+ * same scratch, so calls that overlap on the GPU (other streams, other
+ * threads) race: serialise them. */
 #define FCC_NOALLOC_MAX_BODIES 16384
 #define FCC_NOALLOC_MAX_CELLS 16384
 fcc_status fcc_build_neighbors_noalloc(int32_t precision, int64_t n, const void* x, const void* y, const void* rmax,

@@ -121,6 +121,7 @@ template <class T> struct Term {
 template <class T> struct BodyTypeT {
     T v0, Dr, Dt, mur, muth, muab;
     bool parent_drag;
+    int maxmode;  // 0: every mode; else modes n > maxmode are held at zero (no reference counterpart)
 };
 
 struct SimBase {
@@ -196,7 +197,9 @@ template <class T> struct Sim final : SimBase {
             const fcc_body_type& bt = p->types[t];
             if (bt.parent_drag != 0 && bt.parent_drag != 1)
                 return fail(FCC_ERR_ARGUMENT, "drag must be :substrate or :parent");
-            types.push_back({(T)bt.v0, (T)bt.Dr, (T)bt.Dt, (T)bt.mu_r, (T)bt.mu_theta, (T)bt.mu_ab, bt.parent_drag == 1});
+            if (bt.maxmode < 0) return fail(FCC_ERR_ARGUMENT, "a body type's maxmode must be >= 0");
+            types.push_back({(T)bt.v0, (T)bt.Dr, (T)bt.Dt, (T)bt.mu_r, (T)bt.mu_theta, (T)bt.mu_ab, bt.parent_drag == 1,
+                             bt.maxmode});
         }
         if (p->nterms < 0 || p->nterms > FCC_MAX_TERMS || (p->nterms > 0 && !p->terms))
             return fail(FCC_ERR_ARGUMENT, "energy terms must be BodyTerms, ContactTerms or BondTerms");
@@ -248,6 +251,8 @@ template <class T> struct Sim final : SimBase {
         nth = p->ntheta;
         if (maxmode < 2) return fail(FCC_ERR_ARGUMENT, "maxmode must be ≥ 2");
         if (!(nth > 2 * maxmode)) return fail(FCC_ERR_ARGUMENT, "nθ must exceed 2·maxmode");
+        for (const BodyTypeT<T>& bt : types)
+            if (bt.maxmode > maxmode) return fail(FCC_ERR_ARGUMENT, "a body type's maxmode exceeds the simulation's");
         nc = 2 * K + 1;
         if (b->ncoef != nc) return fail(FCC_ERR_DIMENSION, "coefficient rows must be odd: [a₀; aₙ; bₙ]");
         double dphi64 = 2 * M_PI / nth;
@@ -354,8 +359,18 @@ template <class T> struct Sim final : SimBase {
     T range_T = 0, contact_range_T = 0;
 
     // ---------------------------------------------------- shape & geometry --
+    // Modes above the body type's maxmode held at zero (a per-type limit the
+    // reference does not have; maxmode = 0 leaves every mode free).
+    void mask_modes(int64_t i) {
+        const int mm = types[type[i] - 1].maxmode;
+        if (mm <= 0) return;
+        T* c = &coef[(size_t)nc * i];
+        for (int m = std::max(mm - 1, 0) + 1; m <= K; ++m) c[m] = c[K + m] = T(0);
+    }
+
     // src/dynamics.jl:44-64
     void enforce_shape(int64_t i) {
+        mask_modes(i);
         T* c = &coef[(size_t)nc * i];
         T s = 0;
         for (int m = 1; m <= K; ++m) s += std::sqrt(c[m] * c[m] + c[K + m] * c[K + m]);

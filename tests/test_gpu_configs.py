@@ -10,7 +10,11 @@ against the CPU oracle with a stated tolerance:
   R0 = 0.5 in a 64 x 64 packing at 0.9, OnTypes tensions 0.01 / 0.05, Overlap
   for every pair, nuclei without self-propulsion): forces on a deformed state,
   FP64 at 1e-12, FP32 against the FP64 oracle at 1e-5 with Heaviside flips
-  excluded and counted, and one FP64 step at 1e-12;
+  excluded and counted, and one FP64 step at 1e-12 — with every mode on both
+  types (the reference's shared modes), and with the nuclei held to modes
+  2..6 (BodyType maxmode, against the oracle with the same limit; 30 noisy
+  FP64 steps at rtol 1e-8 and equal rebuild counts, and the nuclei's modes
+  7..10 exactly zero after an FP32 run);
 - the N = 65536 polydisperse monolayer (256 x 256): one evaluation of the
   forces of a deformed FP32 state against the FP64 oracle at 1e-5, flips
   excluded and counted.
@@ -87,10 +91,11 @@ def test_plain_n1024_fp64_trajectory_matches_oracle():
 
 
 # ------------------------------------------------------------ cells + nuclei
-def nuclei_config(T, drag="substrate"):
-    cells, box = fcc.hexagonal_monolayer(64, 64, packing=0.9, maxmode=10, rng=1234)
+def nuclei_config(T, drag="substrate", nucleus_maxmode=0, side=64):
+    cells, box = fcc.hexagonal_monolayer(side, side, packing=0.9, maxmode=10, rng=1234)
     bodies = fcc.with_nuclei(cells, ratio=0.5)
-    kw = dict(types=(fcc.BodyType(v0=0.06, Dr=0.01, μab=0.1), fcc.BodyType(v0=0.0, drag=drag, μab=0.1)),
+    kw = dict(types=(fcc.BodyType(v0=0.06, Dr=0.01, μab=0.1),
+                     fcc.BodyType(v0=0.0, drag=drag, μab=0.1, maxmode=nucleus_maxmode)),
               energies=(fcc.OnTypes(fcc.Tension(0.01), 1), fcc.OnTypes(fcc.Tension(0.05), 2), fcc.Overlap(1.0)),
               dt=0.005, seed=1234, T=T)
     return bodies, box, kw
@@ -159,3 +164,43 @@ def test_n65536_fp32_forces_vs_oracle():
     for f in FIELDS:
         assert relerr(getattr(g.grad, f), getattr(o.grad, f), ~flip) < 1e-5, f
     assert math.isfinite(float(np.asarray(g.grad.Ebody).sum()))
+
+
+# --------------------------------------------- nuclei held to modes 2..6
+def test_nuclei_modes_2_to_6_match_the_masked_oracle(nuclei_state):
+    state, box = nuclei_state
+    _, _, kw = nuclei_config(np.float64, nucleus_maxmode=6)
+    g, o = G(state, box, **kw).refresh(), O(state, box, **kw).refresh()
+    for f in FIELDS:
+        assert relerr(getattr(g.grad, f), getattr(o.grad, f)) < 1e-12, f
+    # the loaded state already has the nuclei's modes 7..10 at zero
+    nuc = state.type == 2
+    assert np.abs(g.bodies.coef[6:10][:, nuc]).max() == 0 and np.abs(g.bodies.coef[15:19][:, nuc]).max() == 0
+
+
+def test_nuclei_modes_2_to_6_short_trajectory_fp64():
+    bodies, box, kw = nuclei_config(np.float64, nucleus_maxmode=6, side=16)
+    bodies.coef[1:] = 0.03 * np.random.default_rng(12).standard_normal((bodies.ncoef - 1, bodies.n))
+    g, o = G(bodies, box, **kw), O(bodies, box, **kw)
+    g.run(30)
+    o.step(30)
+    bg, bo = g.bodies, o.bodies
+    assert np.allclose(bg.x, bo.x, rtol=1e-8) and np.allclose(bg.θ, bo.θ, rtol=1e-8)
+    assert np.allclose(bg.coef, bo.coef, rtol=1e-8, atol=1e-12)
+    assert g.builds == o.builds
+    nuc = bodies.type == 2
+    for b in (bg, bo):
+        assert np.abs(b.coef[6:10][:, nuc]).max() == 0 and np.abs(b.coef[15:19][:, nuc]).max() == 0
+        assert np.abs(b.coef[6:10][:, ~nuc]).max() > 0  # the cells keep every mode
+
+
+def test_nuclei_modes_2_to_6_stay_zero_in_fp32():
+    bodies, box, kw = nuclei_config(np.float32, nucleus_maxmode=6)
+    sim = G(bodies, box, **kw)
+    sim.run(200)
+    b = sim.bodies
+    nuc = b.type == 2
+    assert np.isfinite(b.coef).all()
+    assert np.abs(b.coef[6:10][:, nuc]).max() == 0 and np.abs(b.coef[15:19][:, nuc]).max() == 0
+    assert np.abs(b.coef[1:6][:, nuc]).max() > 0
+    assert np.allclose(fcc.areas(sim), math.pi * np.asarray(bodies.R0, np.float32).astype(float) ** 2, rtol=2e-5)

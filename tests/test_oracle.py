@@ -394,3 +394,30 @@ def test_argument_errors():
         with pytest.raises(fcc.ArgumentError):
             O(fcc.Bodies.new([1.0, 2.0, 3.0], [1.0, 2.0, 3.0], np.zeros(3), np.hstack([coef, coef[:, :1]]), np.ones(3)),
               box, types=(fcc.BodyType(),), energies=(fcc.HarmonicBond(1.0),), bonds=bonds)
+
+
+def test_type_maxmode_equals_a_simulation_with_fewer_modes():
+    """A body type limited to modes 2..6 inside a modes-2..10 simulation is
+    the same dynamics as a modes-2..6 simulation: the masked modes enter as
+    zero (even when given) and stay zero.  Every type limited here, so the
+    two runs are comparable body for body (FP64, 40 noisy steps, 1e-12)."""
+    cells, box = fcc.hexagonal_monolayer(4, 4, packing=0.95, maxmode=10, rng=5)
+    b10 = fcc.with_nuclei(cells, ratio=0.5)
+    b10.coef[1:] = 0.03 * np.random.default_rng(6).standard_normal((18, b10.n))
+    b6 = b10.copy()
+    b6.coef = np.asfortranarray(np.vstack([b10.coef[:1], b10.coef[1:6], b10.coef[10:15]]))
+    def kw(mm):
+        return dict(types=(fcc.BodyType(v0=0.1, Dr=0.05, μab=0.2, maxmode=mm),
+                           fcc.BodyType(drag="parent", μab=0.2, maxmode=mm)),
+                    energies=(fcc.Tension(0.05), fcc.Overlap(1.0)), seed=4)
+    a = oracle.OracleSimulation(b10, box, **kw(6)).step(40)
+    c = oracle.OracleSimulation(b6, box, **kw(0)).step(40)
+    ba, bc = a.bodies, c.bodies
+    assert np.abs(ba.coef[6:10]).max() == 0 and np.abs(ba.coef[15:19]).max() == 0
+    for f in ("x", "y", "θ"):
+        assert np.allclose(getattr(ba, f), getattr(bc, f), rtol=1e-12, atol=1e-12), f
+    assert np.allclose(np.vstack([ba.coef[:6], ba.coef[10:15]]), bc.coef, rtol=1e-12, atol=1e-14)
+    with pytest.raises(fcc.ArgumentError):
+        oracle.OracleSimulation(b6, box, **kw(7))
+    with pytest.raises(fcc.ArgumentError):
+        fcc.BodyType(maxmode=-1)

@@ -1,9 +1,9 @@
 """The neighbour build that allocates no device memory.
 
 fcc_build_neighbors_noalloc exists for callers that cannot call cudaMalloc
-(code inside stream capture, under a memory pool or allocator they do not own,
-or with a device budget fixed up front): they hand it arrays already on the
-device and it keeps its scratch in a static device array of the library.  This
+(code under a memory pool or allocator it does not own, or with a device
+budget fixed up front): they hand it arrays already on the device and it
+keeps its scratch in a static device array of the library.  This
 test allocates its own device buffers (with torch, on the test's side), calls
 the entry point through the C ABI, and checks it against fcc_build_neighbors,
 the allocating entry point, on two calls in a row: integer outputs, so the
@@ -40,7 +40,7 @@ def case(seed, n, Lx, Ly, T):
     return x, y, rmax
 
 
-def run_noalloc(x, y, rmax, Lx, Ly, cutoff, rng_, cap, T):
+def run_noalloc(x, y, rmax, Lx, Ly, cutoff, rng_, cap, T, stream=None):
     import torch
     lib, f = noalloc_fn()
     n = len(x)
@@ -52,8 +52,11 @@ def run_noalloc(x, y, rmax, Lx, Ly, cutoff, rng_, cap, T):
     out = {k: torch.full((m,), -7, dtype=torch.int32, device=dev)
            for k, m in (("cellid", n), ("perm", n), ("start", ncx * ncy), ("stop", ncx * ncy), ("idx", n * cap),
                         ("count", n))}
+    if stream is not None:  # the inputs were written on the current stream
+        stream.wait_stream(torch.cuda.current_stream())
     st = f(32 if T == np.float32 else 64, n, dx.data_ptr(), dy.data_ptr(), dr.data_ptr(), Lx, Ly, cutoff, rng_, cap,
-           *(out[k].data_ptr() for k in ("cellid", "perm", "start", "stop", "idx", "count")), None)
+           *(out[k].data_ptr() for k in ("cellid", "perm", "start", "stop", "idx", "count")),
+           None if stream is None else stream.cuda_stream)
     assert st == 0, lib.fcc_last_error()
     torch.cuda.synchronize()
     h = {k: v.cpu().numpy() for k, v in out.items()}
@@ -79,3 +82,34 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     st = f(64, MAX_BODIES + 1, *([None] * 3), 100.0, 100.0, 4.0, 0.3, 8, *([None] * 6), None)
     assert st == fcc.abi.FCC_ERR_ARGUMENT
     assert b"FCC_NOALLOC_MAX_BODIES" in lib.fcc_last_error()
+
+
+def test_noalloc_on_a_side_stream_with_list_overflow():
+    """Queued on a non-default stream, with a capacity below the largest
+    neighbour count: counts beyond cap are reported as the allocating build
+    reports them, and only the first cap entries are stored."""
+    import torch
+    T = np.float32
+    cutoff = 2 * 1.4 * (1 + np.sqrt(2 / 3)) + 0.3
+    x, y, rmax = case(7, 3000, 60.0, 50.0, T)
+    side = torch.cuda.Stream()
+    cap = 4
+    a = run_noalloc(x, y, rmax, 60.0, 50.0, cutoff, 0.3, cap, T, stream=side)
+    b = fcc.build_neighbors(x.astype(np.float64), y.astype(np.float64), rmax.astype(np.float64), 60.0, 50.0, cutoff,
+                            0.3, cap, T)
+    assert b[5].max() > cap  # the overflow case
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v)
+
+
+def test_noalloc_rejects_a_cutoff_or_box_that_is_not_finite_positive():
+    lib, f = noalloc_fn()
+    for Lx, cutoff in ((100.0, 0.0), (100.0, -1.0), (100.0, float("nan")), (100.0, float("inf")),
+                       (float("nan"), 4.0), (-5.0, 4.0)):
+        st = f(64, 10, *([None] * 3), Lx, 100.0, cutoff, 0.3, 8, *([None] * 6), None)
+        assert st == fcc.abi.FCC_ERR_ARGUMENT, (Lx, cutoff)
+        assert b"finite positive" in lib.fcc_last_error(), (Lx, cutoff)
+    # a tiny cutoff gives a grid far beyond the scratch: rejected before any device work
+    st = f(64, 10, *([None] * 3), 100.0, 100.0, 1e-30, 0.3, 8, *([None] * 6), None)
+    assert st == fcc.abi.FCC_ERR_ARGUMENT
+    assert b"FCC_NOALLOC_MAX_CELLS" in lib.fcc_last_error()
