@@ -123,6 +123,7 @@ struct DevPtrs {
     GridSync* sync;
     const T* cs;     // cos/sin of the node angles, 2*nth
     const T* basis;  // [nth][KM][4]: cos n phi_k, sin n phi_k, n cos n phi_k, n sin n phi_k (n = 2..10)
+    const float* mtab;  // FP32: tensor-core fragment table of the contour contractions (null: none)
     // forces of the split (parent drag) step and of compute_gradients
     T* gx;
     T* gy;

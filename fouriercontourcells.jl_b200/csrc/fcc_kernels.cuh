@@ -633,9 +633,15 @@ constexpr int BASIS_NODES = 40;
 #ifndef FCC_MODE_TABLE
 #define FCC_MODE_TABLE 2  // 1: synthesis reads the table, 2: pullback (measured fastest), 3: both
 #endif
+// Fragments of the tensor-core contractions (below), staged after the mode
+// table: 9 synthesis tiles and 10 pullback tiles, each a TF32 high part and
+// a TF32 remainder, 32 lanes x 4 values.
+constexpr int MMA_SYN_TILES = 9;   // 3 node tiles (48 rows) x 3 coefficient tiles (24 columns)
+constexpr int MMA_PB_TILES = 10;   // 2 coefficient tiles (32 rows) x 5 node tiles (40 columns)
+constexpr int MMA_TABLE_FLOATS = (MMA_SYN_TILES + MMA_PB_TILES) * 2 * 32 * 4;
 template <class T>
 __host__ __device__ constexpr size_t basis_table_bytes() {
-    return sizeof(T) == 4 ? (size_t)BASIS_NODES * KM * 4 * sizeof(T) : 0;
+    return sizeof(T) == 4 ? (size_t)BASIS_NODES * KM * 4 * sizeof(T) + (size_t)MMA_TABLE_FLOATS * sizeof(float) : 0;
 }
 
 // Per warp: the own records of its 32/L bodies, then NBMAX neighbour
@@ -658,6 +664,171 @@ __host__ __device__ constexpr size_t walk_bytes_per_warp() {
 template <class T, int L>
 __host__ __device__ constexpr size_t stage_bytes_per_warp() {
     return (size_t)(32 / L) * (1 + NBMAX) * RECW * sizeof(T) + desc_slot_bytes<T>() + walk_bytes_per_warp<T, L>();
+}
+
+// ------------------------------------------------ tensor-core contractions
+// FP32 kernels of 8 lanes x 5 node slots with one 40-node chunk run the
+// dense contour contractions of a warp's 4 bodies on the tensor cores
+// (mma.sync m16n8k8, TF32 inputs, FP32 accumulation):
+//   pullback    [g_b | h_b] (coefficients x 8) = A^T (32 x 40) . [GR_b | GD_b]
+//     (40 x 8, columns 2b and 2b + 1 of body b), and glab = g + D h with D
+//     the derivative's coefficient map (alpha_m: -n h[beta_m], beta_m:
+//     +n h[alpha_m]): S' Gall of src/gradients.jl:374-386 with the R'' rows
+//     empty, summed over all the body's nodes at once (no lane reductions);
+//   synthesis   [R_b | R'_b] (nodes x 8) = A (48 x 24) . [c_b | c'_b] (24 x 8)
+//     (FCC_MMA_SYNTH = 1), c the R0-scaled lab coefficients of the record
+//     and c' = (0, n beta, -n alpha) the derivative's, so R' = A . c'
+//     (src/geometry.jl:113-122, 248-257).
+// A[k][j] = 1, cos n phi_k, sin n phi_k for coefficient j in record order
+// (a0, alpha_2, beta_2, ...).  Each operand is split into a TF32 high part
+// and a TF32 remainder and the product taken as lo.hi + hi.lo + hi.hi in
+// separate accumulators (the lo.lo term, ~2^-22 relative, dropped): FP32-level
+// accuracy from TF32 units, with dependency chains one k-tile long per term.
+// The tiles pass between the fragment layout and the lanes' node slots
+// through the warp's walk-slot shared memory as (column 2b, 2b + 1) float2
+// pairs, rows of 8 floats with the columns of rows 4..7 (mod 8) rotated by 4
+// words: conflict-free both ways.
+#ifndef FCC_MMA_SYNTH
+#define FCC_MMA_SYNTH 0  // 1: contour synthesis on the tensor cores too (measured: slower, see DESIGN)
+#endif
+
+__device__ __forceinline__ uint32_t tf32_rna(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ void tf32_split(float x, uint32_t& hi, uint32_t& lo) {
+    hi = tf32_rna(x);
+    lo = tf32_rna(x - __uint_as_float(hi));  // x - hi is exact in FP32
+}
+__device__ __forceinline__ void mma_tf32(float (&c)[4], const uint4& a, uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a.x), "r"(a.y), "r"(a.z), "r"(a.w), "r"(b0), "r"(b1));
+}
+// A fragment of `tile` (split 0: high, 1: remainder) for this lane
+__device__ __forceinline__ uint4 mma_frag(const float* mtab, int tile, int split, int lane) {
+    return *reinterpret_cast<const uint4*>(mtab + ((size_t)(tile * 2 + split) * 32 + lane) * 4);
+}
+// word offset of the (column 2b, 2b + 1) pair of row r in the transposition buffer
+__device__ __forceinline__ int mma_pair(int r, int b) { return r * 8 + ((2 * b + 4 * ((r >> 2) & 1)) & 7); }
+// word offset of element (r, column c)
+__device__ __forceinline__ int mma_elem(int r, int c) { return r * 8 + ((c + 4 * ((r >> 2) & 1)) & 7); }
+
+// Contour synthesis of the warp's 4 bodies on the tensor cores: R, R' at the
+// lane's 5 node slots (node l + 8 s of body lane / 8).  own: the 4 staged own
+// records; buf: 48 x 8 floats of warp scratch.
+__device__ __forceinline__ void synth_mma(const float* own, float* buf, const float* mtab, int lane, float (&R)[5],
+                                          float (&R1)[5]) {
+    const int gid = lane >> 2, tig = lane & 3;
+    const float* rec = own + (gid >> 1) * RECW + R_A0;  // B column gid: body gid / 2, derivative if odd
+    const bool deriv = gid & 1;
+    uint32_t bh[3][2], bl[3][2];
+#pragma unroll
+    for (int kt = 0; kt < 3; ++kt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int j = kt * 8 + tig + 4 * h;
+            float v = 0.f;
+            if (j < NCM) {
+                if (!deriv) {
+                    v = rec[j];
+                } else if (j > 0) {  // alpha_m at j = 1 + 2m, beta_m at j = 2 + 2m; n = m + 2
+                    const float n = (float)(((j - 1) >> 1) + 2);
+                    v = (j & 1) ? n * rec[j + 1] : -n * rec[j - 1];
+                }
+            }
+            tf32_split(v, bh[kt][h], bl[kt][h]);
+        }
+    float big[3][4], small[3][4];
+#pragma unroll
+    for (int mt = 0; mt < 3; ++mt)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) big[mt][i] = small[mt][i] = 0.f;
+#pragma unroll
+    for (int kt = 0; kt < 3; ++kt)
+#pragma unroll
+        for (int mt = 0; mt < 3; ++mt) {
+            const int tile = mt * 3 + kt;
+            const uint4 ah = mma_frag(mtab, tile, 0, lane), al = mma_frag(mtab, tile, 1, lane);
+            mma_tf32(small[mt], al, bh[kt][0], bh[kt][1]);
+            mma_tf32(small[mt], ah, bl[kt][0], bl[kt][1]);
+            mma_tf32(big[mt], ah, bh[kt][0], bh[kt][1]);
+        }
+    __syncwarp();  // every lane is done with the buffer's previous contents
+#pragma unroll
+    for (int mt = 0; mt < 3; ++mt) {  // rows gid, gid + 8 of the tile; the (R, R') pair of body tig
+        const int r0 = 16 * mt + gid;
+        *reinterpret_cast<float2*>(buf + mma_pair(r0, tig)) =
+            make_float2(small[mt][0] + big[mt][0], small[mt][1] + big[mt][1]);
+        *reinterpret_cast<float2*>(buf + mma_pair(r0 + 8, tig)) =
+            make_float2(small[mt][2] + big[mt][2], small[mt][3] + big[mt][3]);
+    }
+    __syncwarp();
+    const int b = lane >> 3, l = lane & 7;
+#pragma unroll
+    for (int sl = 0; sl < 5; ++sl) {
+        const float2 v = *reinterpret_cast<const float2*>(buf + mma_pair(l + 8 * sl, b));
+        R[sl] = v.x;
+        R1[sl] = v.y;
+    }
+    __syncwarp();  // the buffer is free again
+}
+
+// Pullback of the warp's 4 bodies on the tensor cores: from GR, GD at the
+// lane's 5 node slots (0 at slots beyond the contour), leaves the (g, h)
+// pairs in buf (32 x 8) for pullback_entry, readable by every lane.
+__device__ __forceinline__ void pullback_mma(const float (&GR)[5], const float (&GD)[5], float* buf,
+                                             const float* mtab, int lane) {
+    const int b = lane >> 3, l = lane & 7;
+    __syncwarp();
+#pragma unroll
+    for (int sl = 0; sl < 5; ++sl)
+        *reinterpret_cast<float2*>(buf + mma_pair(l + 8 * sl, b)) = make_float2(GR[sl], GD[sl]);
+    __syncwarp();
+    const int gid = lane >> 2, tig = lane & 3;
+    float big[2][4], small[2][4];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) big[mt][i] = small[mt][i] = 0.f;
+#pragma unroll
+    for (int kt = 0; kt < 5; ++kt) {  // B rows (nodes) 8 kt + tig and + 4, column gid
+        uint32_t b0h, b0l, b1h, b1l;
+        tf32_split(buf[mma_elem(8 * kt + tig, gid)], b0h, b0l);
+        tf32_split(buf[mma_elem(8 * kt + tig + 4, gid)], b1h, b1l);
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            const int tile = MMA_SYN_TILES + mt * 5 + kt;
+            const uint4 ah = mma_frag(mtab, tile, 0, lane), al = mma_frag(mtab, tile, 1, lane);
+            mma_tf32(small[mt], al, b0h, b1h);
+            mma_tf32(small[mt], ah, b0l, b1l);
+            mma_tf32(big[mt], ah, b0h, b1h);
+        }
+    }
+    __syncwarp();  // every lane has read its B fragments
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {  // rows (coefficients) gid, gid + 8; the (g, h) pair of body tig
+        const int r0 = 16 * mt + gid;
+        *reinterpret_cast<float2*>(buf + mma_pair(r0, tig)) =
+            make_float2(small[mt][0] + big[mt][0], small[mt][1] + big[mt][1]);
+        *reinterpret_cast<float2*>(buf + mma_pair(r0 + 8, tig)) =
+            make_float2(small[mt][2] + big[mt][2], small[mt][3] + big[mt][3]);
+    }
+    __syncwarp();
+}
+// glab entry r (engine order [a0; alpha_2..alpha_10; beta_2..beta_10]) of
+// body b from the pullback buffer
+__device__ __forceinline__ float pullback_entry(const float* buf, int b, int r) {
+    if (r == 0) return buf[mma_pair(0, b)];
+    const bool alpha = r <= KM;
+    const int m = alpha ? r - 1 : r - 1 - KM;
+    const float n = (float)(m + 2);
+    const float2 pa = *reinterpret_cast<const float2*>(buf + mma_pair(1 + 2 * m, b));  // (g, h) of alpha_m
+    const float2 pb = *reinterpret_cast<const float2*>(buf + mma_pair(2 + 2 * m, b));  // (g, h) of beta_m
+    return alpha ? pa.x - n * pb.y : pb.x + n * pa.y;
 }
 
 // Operands of the update loaded early (their latency overlaps the force
@@ -752,15 +923,34 @@ __device__ __forceinline__ void substrate_displacement(const DevPtrs<T>& d, cons
     oy = dt * (P.v0[tc] * so - P.mur[tc] * fy) + sig * x2;
 }
 
+// The lab-frame gradients a lane's update needs: gA[u], gB[u] = dE/dalpha,
+// dE/dbeta of its modes m = l + L u, from the full group-reduced glab row.
+template <class T, int L>
+__device__ __forceinline__ void lane_mode_grads(const T (&gl)[NCM], int l, T (&gA)[UpdatePre<T, L>::MPL],
+                                                T (&gB)[UpdatePre<T, L>::MPL]) {
+#pragma unroll
+    for (int u = 0; u < UpdatePre<T, L>::MPL; ++u) {
+        const int m = l + u * L;
+        T ga = gl[1], gb = gl[1 + KM];
+#pragma unroll
+        for (int mm = 1; mm < KM; ++mm)
+            if (mm == m) ga = gl[1 + mm], gb = gl[1 + KM + mm];
+        gA[u] = ga;
+        gB[u] = gb;
+    }
+}
+
 // Euler-Maruyama update of body g by the L lanes of its group
 // (src/dynamics.jl:128-203 with frame = true): body-frame gradient, theta and
 // shape update, shape bound projection and a0 (FP64 accumulation), wrap,
-// lab frame of the new state into rec[next], skin check.  fx, fy, tt and gl
-// are the group-reduced gradients (uniform across the group).
+// lab frame of the new state into rec[next], skin check.  fx, fy, tt and gl0
+// (dE/da0 of the lab frame / R0) are uniform across the group; gA, gB are the
+// lab-frame mode gradients of the lane's modes (lane_mode_grads).
 template <class T, int L>
 __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T>& P, bool act, int g, int s, int l,
                                             int par, long long clk, T xo, T yo, T wo, T tho, T r0, int ti, T fx, T fy,
-                                            T tt, const T (&gl)[NCM], const UpdatePre<T, L>& pre, int fl,
+                                            T tt, T gl0, const T (&gA)[UpdatePre<T, L>::MPL],
+                                            const T (&gB)[UpdatePre<T, L>::MPL], const UpdatePre<T, L>& pre, int fl,
                                             const T (&nz)[2], bool split, int* rbp) {
     constexpr unsigned FULL = 0xffffffffu;
     constexpr int MPL = UpdatePre<T, L>::MPL;
@@ -779,7 +969,7 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
 
     T* cf = d.coef + (size_t)(act ? g : 0) * NCM;
     const T a0 = pre.a0;
-    const T ga0 = r0 * gl[0];
+    const T ga0 = r0 * gl0;
     const T h0 = ga0 / (T(2) * a0);  // dE/da0 * da0/da_n = -h0 a_n (area constraint)
     const T dtmu = dt * P.muab[ti];
     const int K = P.K;
@@ -792,12 +982,7 @@ __device__ __forceinline__ void update_body(const DevPtrs<T>& d, const SimDesc<T
         an[u] = T(0);
         bn[u] = T(0);
         if (m < Kt) {
-            T ga = gl[1], gb = gl[1 + KM];
-#pragma unroll
-            for (int mm = 1; mm < KM; ++mm)
-                if (mm == m) ga = gl[1 + mm], gb = gl[1 + KM + mm];
-            ga *= r0;
-            gb *= r0;
+            const T ga = gA[u] * r0, gb = gB[u] * r0;
             T so, co;
             cis_pow(co1, so1, m + 2, co, so);
             const T a = pre.a[u], b = pre.b[u];
@@ -931,6 +1116,10 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
     constexpr bool USE_TAB = ONE && sizeof(T) == 4;
     constexpr bool TAB_SYNTH = USE_TAB && (FCC_MODE_TABLE & 1);
     constexpr bool TAB_PULL = USE_TAB && (FCC_MODE_TABLE & 2);
+    // FP32, 8 lanes x 5 node slots, one chunk: synthesis and pullback on the tensor cores
+    constexpr bool MMA = ONE && sizeof(T) == 4 && L == 8 && S == 5;
+    constexpr bool MMA_S = MMA && FCC_MMA_SYNTH;
+    constexpr int MPL = UpdatePre<T, L>::MPL;
     const int lane = threadIdx.x & 31;
     const int l = lane & (L - 1);
     const int g = wg * BPW + lane / L;
@@ -1022,10 +1211,30 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
     unsigned vmask = 0;
     const int nch = ONE ? 1 : (nth + L * S - 1) / (L * S);
 
+    // the warp's walk slots: also the transposition buffer of the tensor-core contractions
+    T* wbase = stage + (size_t)BPW * (1 + NBMAX) * RECW + desc_slot_bytes<T>() / sizeof(T);
+    const float* mtab = MMA ? reinterpret_cast<const float*>(tab) + BASIS_NODES * KM * 4 : nullptr;
+
     // own lab coefficients are read from the staged record (modes outer,
     // nodes inner; per node the same operations as one recurrence per node)
     auto synth = [&](int ch) {
         vmask = 0;
+        if constexpr (MMA_S) {
+#pragma unroll
+            for (int sl = 0; sl < S; ++sl) {
+                const int k = l + L * sl;
+                const bool v = k < nth;
+                C1[sl] = v ? __ldg(d.cs + 2 * k) : T(1);
+                S1[sl] = v ? __ldg(d.cs + 2 * k + 1) : T(0);
+                if (v) vmask |= 1u << sl;
+            }
+            synth_mma(reinterpret_cast<const float*>(stage), reinterpret_cast<float*>(wbase), mtab, lane,
+                      reinterpret_cast<float(&)[5]>(R), reinterpret_cast<float(&)[5]>(R1));
+#pragma unroll
+            for (int sl = 0; sl < S; ++sl)
+                if (!(vmask & (1u << sl))) R[sl] = R1[sl] = T(0);
+            return;
+        }
         T cc[S], ss[S];
 #pragma unroll
         for (int sl = 0; sl < S; ++sl) {
@@ -1114,6 +1323,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
     const T Lx = P.Lx, Ly = P.Ly, iLx = P.invLx, iLy = P.invLy, crange = P.crange;
     const bool rewrap = P.rewrap != 0;
 
+    T GRs[S], GDs[S];  // node gradients of the tensor-core pullback (0 beyond the contour; one chunk)
     for (int ch = 0; ch < nch; ++ch) {
         if (!ONE) synth(ch);
         T p[S];
@@ -1232,13 +1442,14 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                 for (int sl = 0; sl < S; ++sl) p[sl] = wsl[sl * 4 + 3];
             }
         }
-        if (ONE) {
+        if (ONE && !MMA) {
 #pragma unroll
             for (int r = 0; r < NCM; ++r) gl[r] = T(0);
         }
         // contour gradients of node k: GR = W R/q + p dphi R, GD = W R'/q, GDD = 0
 #pragma unroll
         for (int sl = 0; sl < S; ++sl) {
+            GRs[sl] = GDs[sl] = T(0);
             if (!(vmask & (1u << sl))) continue;
             const T r = R[sl], r1 = R1[sl], c1 = C1[sl], s1 = S1[sl];
             T q, iq;
@@ -1249,6 +1460,10 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
             fx += pw * (r * c1 + r1 * s1);
             fy += pw * (r * s1 - r1 * c1);
             tt += (-pw * r) * r1;
+            if constexpr (MMA) {
+                GRs[sl] = GRk;
+                GDs[sl] = GDk;
+            } else {
             gl[0] += GRk;
             if constexpr (TAB_PULL) {
                 const int k = l + L * sl;
@@ -1270,6 +1485,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                     gl[1 + KM + m] += sn * GRk + n * c * GDk;
                 }
             }
+            }
             if (MODE == MODE_DIAG && act) {
                 const int k = ch * L * S + l + L * sl;
                 const size_t o = (size_t)g * nth + k;
@@ -1281,11 +1497,34 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
         }
     }
 
+    if constexpr (MMA) {
+        pullback_mma(reinterpret_cast<const float(&)[5]>(GRs), reinterpret_cast<const float(&)[5]>(GDs),
+                     reinterpret_cast<float*>(wbase), mtab, lane);
+    } else {
+        (void)GRs;
+        (void)GDs;
+    }
     fx = group_sum<L>(fx);
     fy = group_sum<L>(fy);
     tt = group_sum<L>(tt);
+    // dE/da0 and the lane's mode gradients of the lab frame (/ R0)
+    T gl0, gA[MPL], gB[MPL];
+    if constexpr (MMA) {
+        const float* pb = reinterpret_cast<const float*>(wbase);
+        const int b = lane / L;
+        gl0 = pullback_entry(pb, b, 0);
 #pragma unroll
-    for (int r = 0; r < NCM; ++r) gl[r] = group_sum<L>(gl[r]);
+        for (int u = 0; u < MPL; ++u) {
+            const int m = l + u * L;
+            gA[u] = m < KM ? pullback_entry(pb, b, 1 + m) : T(0);
+            gB[u] = m < KM ? pullback_entry(pb, b, 1 + KM + m) : T(0);
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < NCM; ++r) gl[r] = group_sum<L>(gl[r]);
+        gl0 = gl[0];
+        lane_mode_grads<T, L>(gl, l, gA, gB);
+    }
 
     // ---- bond forces on the centre (every lane of the body, no shuffles)
     if (act && P.nbd > 0) {
@@ -1325,25 +1564,25 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
             }
 #pragma unroll
             for (int r = 0; r < NCM; ++r)
-                if ((r & (L - 1)) == l) d.glab[(size_t)g * NCM + r] = gl[r];
+                if ((r & (L - 1)) == l) {
+                    T v;
+                    if constexpr (MMA) v = pullback_entry(reinterpret_cast<const float*>(wbase), lane / L, r);
+                    else v = gl[r];
+                    d.glab[(size_t)g * NCM + r] = v;
+                }
         }
         if (MODE == MODE_DIAG && act) {
             // body-frame gradient gcoef (src/gradients.jl:347-362), frame = true
             const T* cf = d.coef + (size_t)g * NCM;
             const T a0 = ldcg(cf);
-            const T ga0 = r0 * gl[0];
+            const T ga0 = r0 * gl0;
             const T h0 = ga0 / (T(2) * a0);
             const T tho = th;
 #pragma unroll
-            for (int u = 0; u < (KM + L - 1) / L; ++u) {
+            for (int u = 0; u < MPL; ++u) {
                 const int m = l + u * L;
                 if (m >= P.K) continue;
-                T ga = gl[1], gb = gl[1 + KM];
-#pragma unroll
-                for (int mm = 1; mm < KM; ++mm)
-                    if (mm == m) ga = gl[1 + mm], gb = gl[1 + KM + mm];
-                ga *= r0;
-                gb *= r0;
+                const T ga = gA[u] * r0, gb = gB[u] * r0;
                 T so, co;
                 t_sincos(T(m + 2) * tho, &so, &co);
                 const T a = ldcg(cf + 1 + m), b = ldcg(cf + 1 + KM + m);
@@ -1364,7 +1603,8 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
         d.E[g] = E;
     }
     if (valid && !act) carry_record_staged<T, L>(d, g, l, par, own);
-    update_body<T, L>(d, P, act, g, s, l, par, clk, xi, yi, wf, th, r0, ti, fx, fy, tt, gl, pre, fl, nz, false, rbp);
+    update_body<T, L>(d, P, act, g, s, l, par, clk, xi, yi, wf, th, r0, ti, fx, fy, tt, gl0, gA, gB, pre, fl, nz, false,
+                      rbp);
 }
 
 // Phase B of the split step: displacement with parent drag + update of the
@@ -1402,8 +1642,10 @@ __device__ __forceinline__ void update_warp_split(const DevPtrs<T>& d, int wg, i
 #pragma unroll
     for (int r = 0; r < NCM; ++r) gl[r] = ldcg(d.glab + (size_t)gg * NCM + r);
     const T fx = ldcg(d.gx + gg), fy = ldcg(d.gy + gg), tt = ldcg(d.gth + gg);
-    update_body<T, L>(d, P, act, g, s, l, par, clk, rv[R_X], rv[R_Y], rv[R_W], rv[R_TH], r0, ti, fx, fy, tt, gl, pre, fl,
-                      nz, true, rbp);
+    T gA[UpdatePre<T, L>::MPL], gB[UpdatePre<T, L>::MPL];
+    lane_mode_grads<T, L>(gl, l, gA, gB);
+    update_body<T, L>(d, P, act, g, s, l, par, clk, rv[R_X], rv[R_Y], rv[R_W], rv[R_TH], r0, ti, fx, fy, tt, gl[0], gA,
+                      gB, pre, fl, nz, true, rbp);
 }
 
 template <class T>
@@ -1538,8 +1780,9 @@ __device__ __forceinline__ unsigned char* block_stage_of() {
     return fcc_smem + basis_table_bytes<T>();
 }
 
-// Copy the mode table of the first min(nth, BASIS_NODES) nodes into shared
-// memory (FP32 single-chunk kernels); returns it, or null when unused.
+// Copy the mode table of the first min(nth, BASIS_NODES) nodes, and after it
+// the tensor-core fragment table, into shared memory (FP32 single-chunk
+// kernels); returns the mode table, or null when unused.
 template <class T, bool ONE>
 __device__ __forceinline__ const T* stage_basis(const DevPtrs<T>& d) {
     extern __shared__ __align__(16) unsigned char fcc_smem[];
@@ -1547,6 +1790,10 @@ __device__ __forceinline__ const T* stage_basis(const DevPtrs<T>& d) {
     T* tab = reinterpret_cast<T*>(fcc_smem);
     const int n = min(d.nth, BASIS_NODES) * KM * 4;
     for (int u = threadIdx.x; u < n; u += blockDim.x) tab[u] = __ldg(d.basis + u);
+    if (d.mtab) {  // the tensor-core fragments follow the mode table
+        float* mt = reinterpret_cast<float*>(fcc_smem) + BASIS_NODES * KM * 4;
+        for (int u = threadIdx.x; u < MMA_TABLE_FLOATS; u += blockDim.x) mt[u] = __ldg(d.mtab + u);
+    }
     __syncthreads();
     return tab;
 }

@@ -10,6 +10,7 @@
 // (:132-142), shape_index & co. -> fcc_shape_index (src/observables.jl:7-18).
 
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
@@ -481,6 +482,57 @@ std::vector<T> mode_table(int nth) {
     return t;
 }
 
+// Round a float to TF32 (10 mantissa bits), to nearest with ties away from
+// zero: the rounding of cvt.rna.tf32.f32.
+float tf32_round(float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    u = (u + 0x1000u) & 0xffffe000u;
+    float r;
+    std::memcpy(&r, &u, 4);
+    return r;
+}
+
+// Fragment table of the tensor-core contour contractions (the A operands of
+// synth_mma and pullback_mma in fcc_kernels.cuh) for an nth-node contour:
+// A[k][j] = 1, cos n phi_k, sin n phi_k for coefficient j in record order
+// (a0, alpha_2, beta_2, ..., alpha_10, beta_10), phi_k = 2 pi k / nth
+// (FourierBasis, src/basis.jl:35-63), zero beyond the contour and beyond
+// the 19 coefficients.  Synthesis tiles (A, 48 x 24) then pullback tiles
+// (A transposed, 32 x 40), each entry stored as a TF32 high part and the TF32
+// rounding of the remainder, in the m16n8k8 A-fragment order: lane (g, t) =
+// (lane / 4, lane % 4) holds rows g, g + 8, g, g + 8 and columns t, t, t + 4,
+// t + 4 of the tile.
+std::vector<float> mma_table(int nth) {
+    auto basis = [&](int node, int j) -> double {
+        if (node >= nth || j >= NCM) return 0.0;
+        if (j == 0) return 1.0;
+        const int m = (j - 1) / 2;
+        const double a = (m + 2) * node * (2 * PI / nth);
+        return (j & 1) ? std::cos(a) : std::sin(a);
+    };
+    std::vector<float> t((size_t)MMA_TABLE_FLOATS, 0.f);
+    auto put = [&](int tile, int lane, int i, double v) {
+        const float hi = tf32_round((float)v);
+        const float lo = tf32_round((float)(v - (double)hi));
+        t[((size_t)(tile * 2) * 32 + lane) * 4 + i] = hi;
+        t[((size_t)(tile * 2 + 1) * 32 + lane) * 4 + i] = lo;
+    };
+    for (int lane = 0; lane < 32; ++lane) {
+        const int g = lane / 4, tq = lane % 4;
+        const int rows[4] = {g, g + 8, g, g + 8}, cols[4] = {tq, tq, tq + 4, tq + 4};
+        for (int i = 0; i < 4; ++i) {
+            for (int mt = 0; mt < 3; ++mt)
+                for (int kt = 0; kt < 3; ++kt)  // synthesis: rows nodes, columns coefficients
+                    put(mt * 3 + kt, lane, i, basis(16 * mt + rows[i], 8 * kt + cols[i]));
+            for (int mt = 0; mt < 2; ++mt)
+                for (int kt = 0; kt < 5; ++kt)  // pullback: rows coefficients, columns nodes
+                    put(MMA_SYN_TILES + mt * 5 + kt, lane, i, basis(8 * kt + cols[i], 16 * mt + rows[i]));
+        }
+    }
+    return t;
+}
+
 struct EngineBase {
     virtual ~EngineBase() = default;
     virtual fcc_status step(int64_t n, bool eager) = 0;
@@ -524,19 +576,28 @@ struct Engine final : EngineBase {
     // device buffers
     DBuf<SimDesc<T>> sims;
     DBuf<T> rec0, rec1, coef, R0, x0, y0, rmax0, cs, basis, gx, gy, gth, glab, E, P, GR, GD, GDD, gcoef;
+    DBuf<float> mtab;  // FP32: tensor-core fragment table
     DBuf<int> imgx, imgy, sim_of, nb_idx, nb_count, cellid, slot, perm, cstart, cstop, ccount, cell_sim, ch_idx,
-        ch_count, bd_idx, bd_count, flags, maxcount;
-    DBuf<long long> clock, builds;
-    DBuf<GridSync> sync;
-    ObsArea obs;  // perimeters / areas / shape indices: reused device and pinned host buffers
-    int ccap = 1, bcap = 1;
-    // pinned read-back of the run state
+        ch_count, bd_idx, bd_count;
+    // run state of the simulation, one device block so that one copy reads it
+    // back (read_status) and one copy writes its head (load_state); builds
+    // last, out of the written head
     struct Status {
         int flags, maxcount;
-        long long clock, builds;
+        long long clock;
         GridSync sync;
+        long long builds;
     };
-    Status* st_h = nullptr;
+    DBuf<Status> dstat;
+    int* flags_d = nullptr;
+    int* maxcount_d = nullptr;
+    long long* clock_d = nullptr;
+    long long* builds_d = nullptr;
+    GridSync* sync_d = nullptr;
+    ObsArea obs;  // perimeters / areas / shape indices: reused device and pinned host buffers
+    int ccap = 1, bcap = 1;
+    Status* st_h = nullptr;  // pinned read-back of the run state
+    Status* up_h = nullptr;  // pinned head written by load_state
     // state exchange with the host (set_state / get_state): the caller's
     // double arrays are copied as they are into one device area (x, y, theta,
     // coefficients in the reference's layout), and converted and repacked on
@@ -548,6 +609,7 @@ struct Engine final : EngineBase {
     ~Engine() override {
         if (stream) cudaStreamSynchronize(stream);
         if (st_h) cudaFreeHost(st_h);
+        if (up_h) cudaFreeHost(up_h);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -586,13 +648,14 @@ struct Engine final : EngineBase {
         d.bcap = bcap;
         d.bd_idx = bd_idx.p;
         d.bd_count = bd_count.p;
-        d.flags = flags.p;
-        d.clock = clock.p;
-        d.builds = builds.p;
-        d.maxcount = maxcount.p;
-        d.sync = sync.p;
+        d.flags = flags_d;
+        d.clock = clock_d;
+        d.builds = builds_d;
+        d.maxcount = maxcount_d;
+        d.sync = sync_d;
         d.cs = cs.p;
         d.basis = basis.p;
+        d.mtab = mtab.p;
         d.gx = gx.p;
         d.gy = gy.p;
         d.gth = gth.p;
@@ -620,6 +683,7 @@ struct Engine final : EngineBase {
         CUDA_TRY(cudaEventCreate(&ev0));
         CUDA_TRY(cudaEventCreate(&ev1));
         CUDA_TRY(cudaMallocHost(&st_h, sizeof(Status)));
+        CUDA_TRY(cudaMallocHost(&up_h, sizeof(Status)));
 
         N = sp.N;
         K = sp.K;
@@ -664,6 +728,7 @@ struct Engine final : EngineBase {
         }
         FCC_TRY(cs.upload(csh, stream));
         FCC_TRY(basis.upload(mode_table<T>(nth), stream));
+        if (sizeof(T) == 4 && nth <= BASIS_NODES) FCC_TRY(mtab.upload(mma_table(nth), stream));
         FCC_TRY(imgx.upload(std::vector<int>(b->imgx, b->imgx + N), stream));
         FCC_TRY(imgy.upload(std::vector<int>(b->imgy, b->imgy + N), stream));
         FCC_TRY(sim_of.alloc(n, stream));
@@ -680,11 +745,12 @@ struct Engine final : EngineBase {
         FCC_TRY(ch_count.upload(chc, stream));
         FCC_TRY(bd_idx.upload(bdi, stream));
         FCC_TRY(bd_count.upload(bdc, stream));
-        FCC_TRY(flags.upload(std::vector<int>{F_ACTIVE | (has_contact ? F_CONTACT : 0)}, stream));
-        FCC_TRY(maxcount.alloc(1, stream));
-        FCC_TRY(clock.alloc(1, stream));
-        FCC_TRY(builds.alloc(1, stream));
-        FCC_TRY(sync.alloc(1, stream));
+        FCC_TRY(dstat.alloc(1, stream));  // zeroed; load_state below writes the head
+        flags_d = &dstat.p->flags;
+        maxcount_d = &dstat.p->maxcount;
+        clock_d = &dstat.p->clock;
+        builds_d = &dstat.p->builds;
+        sync_d = &dstat.p->sync;
 
         std::vector<int> w(n);
         for (size_t i = 0; i < n; ++i) w[i] = ((parent_h[i] - 1) << 3) | (type_h[i] - 1);
@@ -799,7 +865,6 @@ struct Engine final : EngineBase {
             if (b->imgy) CUDA_TRY(cudaMemcpyAsync(imgy.p, b->imgy, n * sizeof(int), cudaMemcpyHostToDevice, stream));
             CUDA_TRY(cudaMemsetAsync(sim_of.p, 0, n * sizeof(int), stream));
         }
-        CUDA_TRY(cudaMemcpyAsync(clock.p, &clock_h, sizeof(long long), cudaMemcpyHostToDevice, stream));
         CUDA_TRY(cudaMemsetAsync(cell_sim.p, 0, (size_t)ncx * ncy * sizeof(int), stream));
         const DevPtrs<T> d = ptrs();
         if (N > 0) {
@@ -808,12 +873,14 @@ struct Engine final : EngineBase {
                                                 w_dev.p);
             CUDA_TRY(cudaGetLastError());
         }
-        // list invalid: the next step (or update_neighbors!) rebuilds
-        const int f = F_ACTIVE | (has_contact ? (F_CONTACT | F_NEED) : 0);
-        CUDA_TRY(cudaMemcpyAsync(flags.p, &f, sizeof(int), cudaMemcpyHostToDevice, stream));
-        GridSync gs{0, 0, 0, has_contact ? 1 : 0};
-        CUDA_TRY(cudaMemcpyAsync(sync.p, &gs, sizeof(GridSync), cudaMemcpyHostToDevice, stream));
-        return sync_stream();  // the caller's arrays are free for reuse on return
+        // clock, and the list invalid: the next step (or update_neighbors!)
+        // rebuilds; one copy of the status head from pinned memory
+        up_h->flags = F_ACTIVE | (has_contact ? (F_CONTACT | F_NEED) : 0);
+        up_h->maxcount = 0;
+        up_h->clock = clock_h;
+        up_h->sync = GridSync{0, 0, 0, has_contact ? 1 : 0, 0};
+        CUDA_TRY(cudaMemcpyAsync(dstat.p, up_h, offsetof(Status, builds), cudaMemcpyHostToDevice, stream));
+        return sync_stream();  // the caller's arrays (and up_h) are free for reuse on return
     }
 
     int par() const { return (int)(gstep & 1); }
@@ -824,11 +891,7 @@ struct Engine final : EngineBase {
     }
 
     fcc_status read_status() {
-        CUDA_TRY(cudaMemcpyAsync(&st_h->flags, flags.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
-        CUDA_TRY(cudaMemcpyAsync(&st_h->maxcount, maxcount.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
-        CUDA_TRY(cudaMemcpyAsync(&st_h->clock, clock.p, sizeof(long long), cudaMemcpyDeviceToHost, stream));
-        CUDA_TRY(cudaMemcpyAsync(&st_h->builds, builds.p, sizeof(long long), cudaMemcpyDeviceToHost, stream));
-        CUDA_TRY(cudaMemcpyAsync(&st_h->sync, sync.p, sizeof(GridSync), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaMemcpyAsync(st_h, dstat.p, sizeof(Status), cudaMemcpyDeviceToHost, stream));
         CUDA_TRY(cudaStreamSynchronize(stream));
         if (st_h->sync.error) return fail(FCC_ERR_DEVICE, "a grid barrier wait timed out in the step kernel");
         return FCC_OK;
@@ -850,9 +913,9 @@ struct Engine final : EngineBase {
         cap = newcap;
         builds_adjust -= 1;  // the overflowed build is repeated
         const int f = (st_h->flags & ~(F_FROZEN | F_VALID | F_REBUILD)) | F_NEED;
-        CUDA_TRY(cudaMemcpyAsync(flags.p, &f, sizeof(int), cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(cudaMemcpyAsync(flags_d, &f, sizeof(int), cudaMemcpyHostToDevice, stream));
         const int one = 1;
-        CUDA_TRY(cudaMemcpyAsync(&sync.p->any_need, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(cudaMemcpyAsync(&sync_d->any_need, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
         return sync_stream();
     }
 
@@ -896,7 +959,7 @@ struct Engine final : EngineBase {
                 for (int64_t q = 0; q < n; ++q) t_h += desc.dt;
                 step_h += n;
                 clock_h += n;
-                CUDA_TRY(cudaMemcpyAsync(clock.p, &clock_h, sizeof(long long), cudaMemcpyHostToDevice, stream));
+                CUDA_TRY(cudaMemcpyAsync(clock_d, &clock_h, sizeof(long long), cudaMemcpyHostToDevice, stream));
                 return sync_stream();
             }
             return FCC_OK;
@@ -1197,8 +1260,8 @@ struct Engine final : EngineBase {
     fcc_status health(int32_t* nonfinite, int32_t* barrier_error) override {
         int f = 0;
         GridSync g{};
-        CUDA_TRY(cudaMemcpyAsync(&f, flags.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
-        CUDA_TRY(cudaMemcpyAsync(&g, sync.p, sizeof(GridSync), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaMemcpyAsync(&f, flags_d, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaMemcpyAsync(&g, sync_d, sizeof(GridSync), cudaMemcpyDeviceToHost, stream));
         FCC_TRY(sync_stream());
         if (nonfinite) *nonfinite = (f & F_NONFINITE) ? 1 : 0;
         if (barrier_error) *barrier_error = g.error ? 1 : 0;

@@ -230,6 +230,7 @@ struct Pool final : PoolBase {
     DBuf<long long> clock, stop, builds;
     DBuf<GridSync> sync;
     DBuf<T> gx, gy, gth, E, glab, cs, basis;
+    DBuf<float> mtab;  // FP32: tensor-core fragment table
     DBuf<MoveRange> moves;
     std::vector<SimDesc<T>> desc_stage;  // host staging of the descriptors a compaction rebases
     // device staging of an admission (bodies, child and bond lists), reused
@@ -347,6 +348,7 @@ struct Pool final : PoolBase {
         }
         FCC_TRY(cs.upload(csh, stream));
         FCC_TRY(basis.upload(mode_table<T>(nth), stream));
+        if (sizeof(T) == 4 && nth <= BASIS_NODES) FCC_TRY(mtab.upload(mma_table(nth), stream));
         slots.assign(nslots, Slot{});
         for (int s = 0; s < nslots; ++s) stop_h[s] = 0;
         return sync_stream();
@@ -399,6 +401,7 @@ struct Pool final : PoolBase {
         d.sync = sync.p;
         d.cs = cs.p;
         d.basis = basis.p;
+        d.mtab = mtab.p;
         d.gx = gx.p;
         d.gy = gy.p;
         d.gth = gth.p;
