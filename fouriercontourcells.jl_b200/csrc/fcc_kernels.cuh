@@ -1993,20 +1993,37 @@ __global__ void k_finish_rebuild(DevPtrs<T> d) {
 // b_2..b_{in_K+1}] (src/basis.jl:10-14), and the record words w = (parent <<
 // 3) | type (0-based).  Each value is rounded to T here, exactly as a
 // host-side conversion would round it.
+// The inputs may be device memory or page-locked host memory the device
+// reads directly (mapped under unified addressing): the block stages its
+// bodies' coefficient rows through shared memory with consecutive threads
+// reading consecutive doubles, so host reads cross PCIe in full lines.
+// ix_in, iy_in (image counters; null: keep the device's) likewise.
+// Launch with INIT_BLOCK threads and init_smem_bytes(in_nc) bytes.
+constexpr int INIT_BLOCK = 256;
+__host__ __device__ constexpr size_t init_smem_bytes(int in_nc) { return (size_t)INIT_BLOCK * in_nc * sizeof(double); }
 template <class T>
-__global__ void k_init(DevPtrs<T> d, int par, int g0, int n, const double* __restrict__ x,
-                       const double* __restrict__ y, const double* __restrict__ th_in,
-                       const double* __restrict__ coef_in, int in_nc, int in_K, const int* __restrict__ w) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(INIT_BLOCK) k_init(DevPtrs<T> d, int par, int g0, int n, const double* __restrict__ x,
+                                                    const double* __restrict__ y, const double* __restrict__ th_in,
+                                                    const double* __restrict__ coef_in, int in_nc, int in_K,
+                                                    const int* __restrict__ w, const int* __restrict__ ix_in,
+                                                    const int* __restrict__ iy_in) {
+    extern __shared__ double s_coef[];
+    const int i0 = blockIdx.x * INIT_BLOCK;
+    const int nb = min(INIT_BLOCK, n - i0);
+    for (int u = threadIdx.x; u < nb * in_nc; u += INIT_BLOCK) s_coef[u] = coef_in[(size_t)i0 * in_nc + u];
+    __syncthreads();
+    const int i = i0 + threadIdx.x;
     if (i >= n) return;
     const int g = g0 + i;
+    if (ix_in) d.imgx[g] = ix_in[i];
+    if (iy_in) d.imgy[g] = iy_in[i];
     const int s = d.sim_of[g];
     const SimDesc<T>& P = d.sims[s];
     const int K = P.K;
     const int wi = w[i];
     const int kt = min(in_K, P.kmax[wi & 7]);  // modes above the body type's maxmode enter as zero
     T c[NCM];
-    const double* ci = coef_in + (size_t)i * in_nc;
+    const double* ci = s_coef + (size_t)threadIdx.x * in_nc;
     c[0] = T(ci[0]);
 #pragma unroll
     for (int m = 0; m < KM; ++m) {
@@ -2092,27 +2109,36 @@ __global__ void k_init(DevPtrs<T> d, int par, int g0, int n, const double* __res
     for (int r = 0; r < NCM; ++r) d.coef[(size_t)g * NCM + r] = c[r];
 }
 
-// get_state on the device: x, y, theta of the current record and the
-// body-frame coefficients of bodies g0 .. g0+n-1, widened to double in the
-// reference's layout (xyt: x[n], y[n], theta[n]; coef_out: out_nc values per
-// body, [a0; a_2..a_{out_K+1}; b_2..b_{out_K+1}]), ready to be copied to the
-// caller's host arrays as they are.
+// get_state on the device: x, y, theta of the current record, the
+// body-frame coefficients and the image counters of bodies g0 .. g0+n-1,
+// widened to double in the reference's layout, written to x, y, th (n each),
+// coef_out (out_nc values per body, [a0; a_2..a_{out_K+1}; b_2..b_{out_K+1}])
+// and ix, iy (null: skipped).  The outputs may be device memory or
+// page-locked host memory the device writes directly: every output is written
+// with consecutive threads on consecutive elements (the coefficients as one
+// flat array), so host writes cross PCIe in full lines.  Grid-stride loops.
 template <class T>
-__global__ void k_store_host(DevPtrs<T> d, int par, int g0, int n, double* __restrict__ xyt,
-                             double* __restrict__ coef_out, int out_nc, int out_K) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int g = g0 + i;
-    const T* rc = rec_cur(d, par) + (size_t)g * RECW;
-    xyt[i] = (double)rc[R_X];
-    xyt[(size_t)n + i] = (double)rc[R_Y];
-    xyt[2 * (size_t)n + i] = (double)rc[R_TH];
-    const T* cf = d.coef + (size_t)g * NCM;
-    double* co = coef_out + (size_t)i * out_nc;
-    co[0] = (double)cf[0];
-    for (int m = 0; m < out_K; ++m) {
-        co[1 + m] = (double)cf[1 + m];
-        co[1 + out_K + m] = (double)cf[1 + KM + m];
+__global__ void k_store_host(DevPtrs<T> d, int par, int g0, int n, double* __restrict__ x, double* __restrict__ y,
+                             double* __restrict__ th, double* __restrict__ coef_out, int out_nc, int out_K,
+                             int* __restrict__ ix, int* __restrict__ iy) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthr = gridDim.x * blockDim.x;
+    const T* rc = rec_cur(d, par);
+    for (int i = tid; i < n; i += nthr) {
+        const T* r = rc + (size_t)(g0 + i) * RECW;
+        if (x) x[i] = (double)r[R_X];
+        if (y) y[i] = (double)r[R_Y];
+        if (th) th[i] = (double)r[R_TH];
+        if (ix) ix[i] = d.imgx[g0 + i];
+        if (iy) iy[i] = d.imgy[g0 + i];
+    }
+    if (coef_out) {
+        const long long tot = (long long)n * out_nc;
+        for (long long u = tid; u < tot; u += nthr) {
+            const int i = (int)(u / out_nc), j = (int)(u - (long long)i * out_nc);
+            // j = 0: a0; 1..out_K: a_{j+1}; out_K+1..2 out_K: b_{j-out_K+1}
+            const int r = j == 0 ? 0 : (j <= out_K ? j : KM + (j - out_K));
+            coef_out[u] = (double)d.coef[(size_t)(g0 + i) * NCM + r];
+        }
     }
 }
 

@@ -124,6 +124,22 @@ struct Stage {
     V* p() const { return buf.p; }
 };
 
+// The device's address of page-locked host memory that the device reads and
+// writes in place (every page-locked allocation is mapped under unified
+// addressing), or null for any other pointer (pageable memory, device
+// memory, null).
+template <class V>
+V* mapped_view(V* p) {
+    if (!p) return nullptr;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();  // not a pointer the runtime knows: not mapped
+        return nullptr;
+    }
+    if (a.type != cudaMemoryTypeHost || !a.devicePointer) return nullptr;
+    return static_cast<V*>(a.devicePointer);
+}
+
 // Device output of k_observables and its pinned host copy, grown on demand
 // and reused: an observable query allocates nothing after the first at its
 // size (allocation and release of device memory synchronise the device and
@@ -846,31 +862,47 @@ struct Engine final : EngineBase {
         return FCC_OK;
     }
 
-    // Copy a host body state in and rebuild the derived geometry (k_init).
-    // The caller's arrays go to the device as they are (a DMA when the caller
-    // passes pinned host memory; the driver stages pageable memory), and
-    // k_init rounds them to T and repacks the coefficients, so the host does
-    // no per-body work.  The call returns once the copies have completed: the
-    // caller may reuse its buffers.
+    // Copy a host body state in and rebuild the derived geometry (k_init),
+    // which rounds the caller's doubles to T and repacks the coefficients on
+    // the device.  Page-locked host arrays are read by k_init in place (one
+    // launch, no copy call); other arrays go to the device as they are, one
+    // copy each (the driver stages pageable memory).  The call returns once
+    // the inputs are no longer needed: the caller may reuse its buffers.
     fcc_status load_state(const fcc_bodies_host* b, int64_t clk) {
         const size_t n = (size_t)N;
         if (clk >= 0) clock_h = clk;
-        double* dx = xch_d.p;
+        const double *px = nullptr, *py = nullptr, *pth = nullptr, *pc = nullptr;
+        const int *pix = nullptr, *piy = nullptr;
         if (n) {
-            CUDA_TRY(cudaMemcpyAsync(dx, b->x, n * sizeof(double), cudaMemcpyHostToDevice, stream));
-            CUDA_TRY(cudaMemcpyAsync(dx + n, b->y, n * sizeof(double), cudaMemcpyHostToDevice, stream));
-            CUDA_TRY(cudaMemcpyAsync(dx + 2 * n, b->theta, n * sizeof(double), cudaMemcpyHostToDevice, stream));
-            CUDA_TRY(cudaMemcpyAsync(dx + 3 * n, b->coef, n * nc * sizeof(double), cudaMemcpyHostToDevice, stream));
-            if (b->imgx) CUDA_TRY(cudaMemcpyAsync(imgx.p, b->imgx, n * sizeof(int), cudaMemcpyHostToDevice, stream));
-            if (b->imgy) CUDA_TRY(cudaMemcpyAsync(imgy.p, b->imgy, n * sizeof(int), cudaMemcpyHostToDevice, stream));
+            px = mapped_view(b->x);
+            py = mapped_view(b->y);
+            pth = mapped_view(b->theta);
+            pc = mapped_view(b->coef);
+            pix = mapped_view(b->imgx);
+            piy = mapped_view(b->imgy);
+            const bool in_place = px && py && pth && pc && (!b->imgx || pix) && (!b->imgy || piy);
+            if (!in_place) {
+                double* dx = xch_d.p;
+                px = dx;
+                py = dx + n;
+                pth = dx + 2 * n;
+                pc = dx + 3 * n;
+                pix = piy = nullptr;
+                CUDA_TRY(cudaMemcpyAsync(dx, b->x, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+                CUDA_TRY(cudaMemcpyAsync(dx + n, b->y, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+                CUDA_TRY(cudaMemcpyAsync(dx + 2 * n, b->theta, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+                CUDA_TRY(cudaMemcpyAsync(dx + 3 * n, b->coef, n * nc * sizeof(double), cudaMemcpyHostToDevice, stream));
+                if (b->imgx) CUDA_TRY(cudaMemcpyAsync(imgx.p, b->imgx, n * sizeof(int), cudaMemcpyHostToDevice, stream));
+                if (b->imgy) CUDA_TRY(cudaMemcpyAsync(imgy.p, b->imgy, n * sizeof(int), cudaMemcpyHostToDevice, stream));
+            }
             CUDA_TRY(cudaMemsetAsync(sim_of.p, 0, n * sizeof(int), stream));
         }
         CUDA_TRY(cudaMemsetAsync(cell_sim.p, 0, (size_t)ncx * ncy * sizeof(int), stream));
         const DevPtrs<T> d = ptrs();
         if (N > 0) {
-            const int grid = (int)((N + 255) / 256);
-            k_init<T><<<grid, 256, 0, stream>>>(d, par(), 0, (int)N, dx, dx + n, dx + 2 * n, dx + 3 * n, nc, K,
-                                                w_dev.p);
+            const int grid = (int)((N + INIT_BLOCK - 1) / INIT_BLOCK);
+            k_init<T><<<grid, INIT_BLOCK, init_smem_bytes(nc), stream>>>(d, par(), 0, (int)N, px, py, pth, pc, nc, K,
+                                                                        w_dev.p, pix, piy);
             CUDA_TRY(cudaGetLastError());
         }
         // clock, and the list invalid: the next step (or update_neighbors!)
@@ -1061,29 +1093,41 @@ struct Engine final : EngineBase {
     }
 
     // sim.bodies: k_store_host widens x, y, theta and the coefficients to
-    // double in the reference's layout on the device; they and the image
-    // counters are copied straight into the caller's arrays (a DMA for pinned
-    // host memory).  R0, type and parent are fixed since create and come from
-    // the host mirror.
+    // double in the reference's layout on the device and writes them, with
+    // the image counters, into the caller's page-locked arrays in place (one
+    // launch), or into the exchange area for one copy per array into other
+    // memory.  R0, type and parent are fixed since create and come from the
+    // host mirror.
     fcc_status get_state(fcc_bodies_host* o, int64_t* clk, double* t, int64_t* stp) override {
         if (o) {
             if (o->n != N || o->ncoef != nc) return fail(FCC_ERR_DIMENSION, "state buffers do not match the simulation");
             const size_t n = (size_t)N;
             if (n) {
-                double* dx = xch_d.p;
-                const int grid = (int)((N + 255) / 256);
-                k_store_host<T><<<grid, 256, 0, stream>>>(ptrs(), par(), 0, (int)N, dx, dx + 3 * n, nc, K);
-                CUDA_TRY(cudaGetLastError());
-                if (o->x) CUDA_TRY(cudaMemcpyAsync(o->x, dx, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
-                if (o->y) CUDA_TRY(cudaMemcpyAsync(o->y, dx + n, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
-                if (o->theta)
-                    CUDA_TRY(cudaMemcpyAsync(o->theta, dx + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
-                if (o->coef)
-                    CUDA_TRY(cudaMemcpyAsync(o->coef, dx + 3 * n, n * nc * sizeof(double), cudaMemcpyDeviceToHost, stream));
-                if (o->imgx) CUDA_TRY(cudaMemcpyAsync(o->imgx, imgx.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
-                if (o->imgy) CUDA_TRY(cudaMemcpyAsync(o->imgy, imgy.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+                double *vx = mapped_view(o->x), *vy = mapped_view(o->y), *vth = mapped_view(o->theta),
+                       *vc = mapped_view(o->coef);
+                int *vix = mapped_view(o->imgx), *viy = mapped_view(o->imgy);
+                const bool in_place = (!o->x || vx) && (!o->y || vy) && (!o->theta || vth) && (!o->coef || vc) &&
+                                      (!o->imgx || vix) && (!o->imgy || viy);
+                const int grid = (int)std::min<int64_t>((N * nc + 255) / 256, (int64_t)nsm * 8);
+                if (in_place) {
+                    k_store_host<T><<<grid, 256, 0, stream>>>(ptrs(), par(), 0, (int)N, vx, vy, vth, vc, nc, K, vix, viy);
+                    CUDA_TRY(cudaGetLastError());
+                } else {
+                    double* dx = xch_d.p;
+                    k_store_host<T><<<grid, 256, 0, stream>>>(ptrs(), par(), 0, (int)N, dx, dx + n, dx + 2 * n, dx + 3 * n,
+                                                              nc, K, nullptr, nullptr);
+                    CUDA_TRY(cudaGetLastError());
+                    if (o->x) CUDA_TRY(cudaMemcpyAsync(o->x, dx, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+                    if (o->y) CUDA_TRY(cudaMemcpyAsync(o->y, dx + n, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+                    if (o->theta)
+                        CUDA_TRY(cudaMemcpyAsync(o->theta, dx + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+                    if (o->coef)
+                        CUDA_TRY(cudaMemcpyAsync(o->coef, dx + 3 * n, n * nc * sizeof(double), cudaMemcpyDeviceToHost, stream));
+                    if (o->imgx) CUDA_TRY(cudaMemcpyAsync(o->imgx, imgx.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+                    if (o->imgy) CUDA_TRY(cudaMemcpyAsync(o->imgy, imgy.p, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+                }
             }
-            // the fixed fields while the copies run
+            // the fixed fields while the device works
             for (size_t i = 0; i < n; ++i) {
                 if (o->R0) o->R0[i] = (double)R0_h[i];
                 if (o->type) o->type[i] = type_h[i];

@@ -519,9 +519,10 @@ struct Pool final : PoolBase {
         CUDA_TRY(cudaMemcpyAsync(dx + 3 * n, b->coef, n * P.nc * sizeof(double), cudaMemcpyHostToDevice, stream));
         FCC_TRY(st_w.upload(w, stream));
         const DevPtrs<T> d = ptrs();
-        const int blocks = (int)((n + 255) / 256);
-        k_init<T><<<blocks, 256, 0, stream>>>(d, par(), (int)S.off, (int)n, dx, dx + n, dx + 2 * n, dx + 3 * n, P.nc,
-                                              P.K, st_w.p());
+        const int blocks = (int)((n + INIT_BLOCK - 1) / INIT_BLOCK);
+        k_init<T><<<blocks, INIT_BLOCK, init_smem_bytes(P.nc), stream>>>(d, par(), (int)S.off, (int)n, dx, dx + n,
+                                                                          dx + 2 * n, dx + 3 * n, P.nc, P.K, st_w.p(),
+                                                                          nullptr, nullptr);
         CUDA_TRY(cudaGetLastError());
         return sync_stream();
     }
@@ -1005,8 +1006,8 @@ struct Pool final : PoolBase {
             if (n > 0) {
                 FCC_TRY(st_xch.reserve(n * (3 + (size_t)P.nc), stream));
                 double* dx = st_xch.p();
-                k_store_host<T><<<(int)((n + 255) / 256), 256, 0, stream>>>(ptrs(), par(), (int)S.off, (int)n, dx,
-                                                                            dx + 3 * n, P.nc, P.K);
+                k_store_host<T><<<(int)std::min<size_t>((n * P.nc + 255) / 256, (size_t)nsm * 8), 256, 0, stream>>>(
+                    ptrs(), par(), (int)S.off, (int)n, dx, dx + n, dx + 2 * n, dx + 3 * n, P.nc, P.K, nullptr, nullptr);
                 CUDA_TRY(cudaGetLastError());
                 if (o->x) CUDA_TRY(cudaMemcpyAsync(o->x, dx, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
                 if (o->y) CUDA_TRY(cudaMemcpyAsync(o->y, dx + n, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
