@@ -15,6 +15,8 @@ The directory name is not a Python identifier; load it with
 
 from .model import (ArgumentError, DimensionMismatch, DeviceError, PoolFull, BodyType, EnergyTerm, BodyTerm, ContactTerm,
                     BondTerm, Tension, PerimeterElasticity, Overlap, LinearRepulsion, HarmonicBond, OnTypes,
+                    UserTerm, UserBodyTerm, UserContactTerm, UserBondTerm, Bending, ShapeIndexElasticity, Adhesion,
+                    QuarticBond,
                     Bodies, PeriodicBox, vcat, nbodies, hexagonal_monolayer, with_nuclei, parent_bonds,
                     polydisperse_monolayer, minimum_image, wrap)
 from .simulation import (Simulation, NativeSimulation, native_library, step, run, compute_gradients,
@@ -32,5 +34,6 @@ __all__ = [
     "polydisperse_monolayer", "minimum_image", "wrap", "Simulation", "NativeSimulation", "native_library", "step",
     "run", "compute_gradients", "update_neighbors", "perimeters", "areas", "shape_index", "body_energy",
     "positions", "unwrapped_positions", "contours", "protrusion", "Gradients", "Geometry", "NeighborInfo",
-    "philox_noise", "build_neighbors", "barrier_selftest", "pinned_bodies", "pinned_copy",
+    "philox_noise", "build_neighbors", "barrier_selftest", "pinned_bodies", "pinned_copy", "UserTerm",
+    "UserBodyTerm", "UserContactTerm", "UserBondTerm", "Bending", "ShapeIndexElasticity", "Adhesion", "QuarticBond",
 ]

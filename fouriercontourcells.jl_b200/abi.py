@@ -14,7 +14,7 @@ import ctypes as C
 import numpy as np
 
 from .model import (ArgumentError, DimensionMismatch, DeviceError, PoolFull, BodyType, Bodies, OnTypes, Tension,
-                    PerimeterElasticity, Overlap, LinearRepulsion, HarmonicBond, is_body_term,
+                    PerimeterElasticity, Overlap, LinearRepulsion, HarmonicBond, UserTerm, is_body_term,
                     is_contact_term, is_bond_term)
 
 MAX_TYPES = 8
@@ -32,7 +32,8 @@ c_int32_p = C.POINTER(C.c_int32)
 class FccTerm(C.Structure):
     _fields_ = [("kind", C.c_int32), ("ntypes_on", C.c_int32), ("types_on", C.c_int32 * MAX_TYPES),
                 ("a", C.c_double), ("b", C.c_double), ("nJ", C.c_int32),
-                ("J", C.c_double * (MAX_TYPES * MAX_TYPES)), ("Jrel", C.c_double * (MAX_TYPES * MAX_TYPES))]
+                ("J", C.c_double * (MAX_TYPES * MAX_TYPES)), ("Jrel", C.c_double * (MAX_TYPES * MAX_TYPES)),
+                ("user", C.c_int32)]
 
 
 class FccBodyType(C.Structure):
@@ -115,6 +116,8 @@ def _term_struct(term) -> FccTerm:
         ft.a = inner.k
     elif isinstance(inner, HarmonicBond):
         ft.a, ft.b = inner.k, inner.r0
+    elif isinstance(inner, UserTerm):
+        ft.a, ft.b, ft.user = inner.a, inner.b, inner.index
     elif isinstance(inner, Overlap):
         J = np.asarray(inner.J, dtype=np.float64)
         R = np.asarray(inner.Jrelated, dtype=np.float64)

@@ -34,6 +34,7 @@ constexpr int NCM = 2 * KM + 1;
 constexpr int RECW = 24;     // record width (values)
 constexpr int MT = 8;        // max body types
 constexpr int MTERM = 16;    // max terms
+constexpr int MUT = 4;       // max compiled user terms of each kind (FCC_MAX_USER_TERMS)
 constexpr double SHAPE_BOUND = 0.816496580927726;  // sqrt(2/3), src/dynamics.jl:26
 
 // record slots
@@ -76,6 +77,11 @@ struct SimDesc {
     T cB[MT];                    // summed LinearRepulsion k of terms applying to ti (k*d at d > 0)
     uint32_t bd_mask[MTERM];
     T bd_k[MTERM], bd_r0[MTERM];
+    // compiled user terms (include/fcc_user_terms.h): table index, type mask, parameters a, b
+    int nub, nuc, nubd;  // body, contact, bond terms
+    int ub_id[MUT], uc_id[MUT], ubd_id[MUT];
+    uint32_t ub_mask[MUT], uc_mask[MUT], ubd_mask[MUT];
+    T ub_a[MUT], ub_b[MUT], uc_a[MUT], uc_b[MUT], ubd_a[MUT], ubd_b[MUT];
 };
 
 struct GridSync {

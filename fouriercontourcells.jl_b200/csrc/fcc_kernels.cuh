@@ -19,6 +19,7 @@
 #include <climits>
 
 #include "fcc_device.cuh"
+#include "../../include/fcc_user_terms.h"
 
 namespace fcc {
 
@@ -1105,7 +1106,10 @@ enum : int { MODE_FUSED = 0, MODE_FORCES = 1, MODE_DIAG = 2 };
 //     LinearRepulsion) and its gradients          391-429; src/gradients.jl:265-307
 //   bond forces                                 src/energies/bonds.jl:98-111
 //   pullback glab = S' Gall                     src/gradients.jl:374-386
-template <class T, int L, int S, bool ONE, int MODE>
+// USER: the simulation has compiled user terms (include/fcc_user_terms.h):
+// R'' is synthesised, user integrals, node gradients (GDD included),
+// pressures and bond gradients are added, and the pullback includes R''.
+template <class T, int L, int S, bool ONE, int MODE, bool USER = false>
 __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stage, int par, const SimDesc<T>* sim0,
                                             const T* tab, int& cached, int* rbp, const BarrierLocal* lone) {
     constexpr int BPW = 32 / L;
@@ -1117,7 +1121,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
     constexpr bool TAB_SYNTH = USE_TAB && (FCC_MODE_TABLE & 1);
     constexpr bool TAB_PULL = USE_TAB && (FCC_MODE_TABLE & 2);
     // FP32, 8 lanes x 5 node slots, one chunk: synthesis and pullback on the tensor cores
-    constexpr bool MMA = ONE && sizeof(T) == 4 && L == 8 && S == 5;
+    constexpr bool MMA = ONE && sizeof(T) == 4 && L == 8 && S == 5 && !USER;
     constexpr bool MMA_S = MMA && FCC_MMA_SYNTH;
     constexpr int MPL = UpdatePre<T, L>::MPL;
     const int lane = threadIdx.x & 31;
@@ -1208,6 +1212,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
     const int pi = wv >> 3;
 
     T R[S], R1[S], C1[S], S1[S];
+    T R2[S];  // R'' (user terms only)
     unsigned vmask = 0;
     const int nch = ONE ? 1 : (nth + L * S - 1) / (L * S);
 
@@ -1248,6 +1253,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
             ss[sl] = s1;
             R[sl] = a0r;
             R1[sl] = T(0);
+            R2[sl] = T(0);
             if (v) vmask |= 1u << sl;
         }
 #pragma unroll
@@ -1267,12 +1273,13 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                     cc[sl] = cn;
                     R[sl] += al * cc[sl] + be * ss[sl];
                     R1[sl] += n * (be * cc[sl] - al * ss[sl]);
+                    if constexpr (USER) R2[sl] -= (n * n) * (al * cc[sl] + be * ss[sl]);
                 }
             }
         }
 #pragma unroll
         for (int sl = 0; sl < S; ++sl)
-            if (!(vmask & (1u << sl))) R[sl] = R1[sl] = T(0);
+            if (!(vmask & (1u << sl))) R[sl] = R1[sl] = R2[sl] = T(0);
     };
 
     cp_async_wait_group<1>();  // the own record (the neighbour copies may still fly)
@@ -1290,6 +1297,27 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
             }
     }
     const T Q = group_sum<L>(Qp) * dphi;
+    // user body terms: integrals Q_j = sum over the nodes of q_j(R, R', R'') dphi
+    T UQ[MUT][fcc_user::MAX_M];
+    if constexpr (USER) {
+        static_assert(ONE, "user terms run in single-chunk kernels");
+#pragma unroll
+        for (int u = 0; u < MUT; ++u) {
+#pragma unroll
+            for (int j = 0; j < fcc_user::MAX_M; ++j) UQ[u][j] = T(0);
+            if (u >= P.nub || !((P.ub_mask[u] >> ti) & 1u)) continue;
+#pragma unroll
+            for (int sl = 0; sl < S; ++sl)
+                if (vmask & (1u << sl)) {
+                    T q[fcc_user::MAX_M] = {};
+                    fcc_user::body_q<T>(P.ub_id[u], R[sl], R1[sl], R2[sl], P.ub_a[u], P.ub_b[u], q);
+#pragma unroll
+                    for (int j = 0; j < fcc_user::MAX_M; ++j) UQ[u][j] += q[j];
+                }
+#pragma unroll
+            for (int j = 0; j < fcc_user::MAX_M; ++j) UQ[u][j] = group_sum<L>(UQ[u][j]) * dphi;
+        }
+    }
 
     // ---- body terms: W = sum_t dF_t/dQ * dphi, E = e_1 + (e_2 + ...)
     T W = T(0), E = T(0);
@@ -1307,6 +1335,21 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
             E = (P.bt_kind[q] == BT_TENSION ? a * Q : a * (dq * dq)) + E;
         }
         W *= dphi;
+    }
+    // user body terms: energies F_u(Q) and node weights UW = dF_u/dQ_j dphi
+    T UW[MUT][fcc_user::MAX_M];
+    if constexpr (USER) {
+#pragma unroll
+        for (int u = 0; u < MUT; ++u) {
+#pragma unroll
+            for (int j = 0; j < fcc_user::MAX_M; ++j) UW[u][j] = T(0);
+            if (u >= P.nub || !((P.ub_mask[u] >> ti) & 1u)) continue;
+            T dF[fcc_user::MAX_M] = {};
+            fcc_user::body_dF<T>(P.ub_id[u], UQ[u], r0, ti + 1, P.ub_a[u], P.ub_b[u], dF);
+#pragma unroll
+            for (int j = 0; j < fcc_user::MAX_M; ++j) UW[u][j] = dF[j] * dphi;
+            E += fcc_user::body_F<T>(P.ub_id[u], UQ[u], r0, ti + 1, P.ub_a[u], P.ub_b[u]);
+        }
     }
 
     // ---- pass 2: contact pressure, contour gradients, force/torque and pullback partials
@@ -1420,6 +1463,13 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                         // pair coupling of the terms (src/energies/contact.jl:267-293)
                         T gv = dd >= T(0) ? cAj : T(0);
                         if (dd > T(0)) gv += P.cB[ti] * dd;
+                        if constexpr (USER) {
+#pragma unroll
+                            for (int u = 0; u < MUT; ++u)
+                                if (u < P.nuc && ((P.uc_mask[u] >> ti) & 1u))
+                                    gv += fcc_user::contact_g<T>(P.uc_id[u], dd, ti + 1, (wjv & 7) + 1, (wjv >> 3) == pi,
+                                                                P.uc_a[u], P.uc_b[u]);
+                        }
                         return gv;
                     };
                     while (hm) {
@@ -1455,8 +1505,23 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
             T q, iq;
             norm_inv(r * r + r1 * r1, q, iq);
             const T pw = p[sl] * dphi;
-            const T GRk = W * r * iq + pw * r;
-            const T GDk = W * r1 * iq;
+            T GRk = W * r * iq + pw * r;
+            T GDk = W * r1 * iq;
+            T GDDk = T(0);
+            if constexpr (USER) {
+#pragma unroll
+                for (int u = 0; u < MUT; ++u) {
+                    if (u >= P.nub || !((P.ub_mask[u] >> ti) & 1u)) continue;
+                    T dq[fcc_user::MAX_M][3] = {};
+                    fcc_user::body_dq<T>(P.ub_id[u], r, r1, R2[sl], P.ub_a[u], P.ub_b[u], dq);
+#pragma unroll
+                    for (int j = 0; j < fcc_user::MAX_M; ++j) {
+                        GRk += UW[u][j] * dq[j][0];
+                        GDk += UW[u][j] * dq[j][1];
+                        GDDk += UW[u][j] * dq[j][2];
+                    }
+                }
+            }
             fx += pw * (r * c1 + r1 * s1);
             fy += pw * (r * s1 - r1 * c1);
             tt += (-pw * r) * r1;
@@ -1470,8 +1535,14 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
 #pragma unroll
                 for (int m = 0; m < KM; ++m) {
                     const auto t = lds4(tab + (k * KM + m) * 4);
-                    gl[1 + m] += t.x * GRk - t.w * GDk;
-                    gl[1 + KM + m] += t.y * GRk + t.z * GDk;
+                    if constexpr (USER) {  // R'' rows: -n^2 cos, -n^2 sin
+                        const T n = T(m + 2);
+                        gl[1 + m] += t.x * GRk - t.w * GDk - (n * t.z) * GDDk;
+                        gl[1 + KM + m] += t.y * GRk + t.z * GDk - (n * t.w) * GDDk;
+                    } else {
+                        gl[1 + m] += t.x * GRk - t.w * GDk;
+                        gl[1 + KM + m] += t.y * GRk + t.z * GDk;
+                    }
                 }
             } else {
                 T c = c1, sn = s1;
@@ -1481,8 +1552,13 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                     const T cn = c * c1 - sn * s1;
                     sn = sn * c1 + c * s1;
                     c = cn;
-                    gl[1 + m] += c * GRk - n * sn * GDk;
-                    gl[1 + KM + m] += sn * GRk + n * c * GDk;
+                    if constexpr (USER) {
+                        gl[1 + m] += c * GRk - n * sn * GDk - (n * n) * c * GDDk;
+                        gl[1 + KM + m] += sn * GRk + n * c * GDk - (n * n) * sn * GDDk;
+                    } else {
+                        gl[1 + m] += c * GRk - n * sn * GDk;
+                        gl[1 + KM + m] += sn * GRk + n * c * GDk;
+                    }
                 }
             }
             }
@@ -1492,7 +1568,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                 d.P[o] = p[sl];
                 d.GR[o] = GRk;
                 d.GD[o] = GDk;
-                d.GDD[o] = T(0);
+                d.GDD[o] = GDDk;
             }
         }
     }
@@ -1527,7 +1603,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
     }
 
     // ---- bond forces on the centre (every lane of the body, no shuffles)
-    if (act && P.nbd > 0) {
+    if (act && (P.nbd > 0 || (USER && P.nubd > 0))) {
         const int bc = __ldg(d.bd_count + g);
         T bx = T(0), by = T(0);
         for (int q = 0; q < bc; ++q) {
@@ -1546,6 +1622,16 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
                 const T f = rr > T(0) ? k * (T(1) - rb / rr) : (rb == T(0) ? k : T(0));
                 a0 = f * d0 + a0;
                 a1 = f * d1 + a1;
+            }
+            if constexpr (USER) {
+#pragma unroll
+                for (int u = 0; u < MUT; ++u) {
+                    if (u >= P.nubd || !((P.ubd_mask[u] >> ti) & 1u) || !((P.ubd_mask[u] >> tj) & 1u)) continue;
+                    T hx, hy;
+                    fcc_user::bond_grad<T>(P.ubd_id[u], d0, d1, ti + 1, tj + 1, P.ubd_a[u], P.ubd_b[u], hx, hy);
+                    a0 += hx;
+                    a1 += hy;
+                }
             }
             bx += a0;
             by += a1;
@@ -1802,7 +1888,7 @@ __device__ __forceinline__ const T* stage_basis(const DevPtrs<T>& d) {
 // Each block takes a contiguous range of warp groups (balanced bodies per SM);
 // within the block the warps take them statically, or (FP32, one simulation)
 // each warp its first and then the block's next untaken one.
-template <class T, int L, int S, bool ONE, bool SPLIT, int BLK, int MINB>
+template <class T, int L, int S, bool ONE, bool SPLIT, int BLK, int MINB, bool USER = false>
 __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, int par0) {
     constexpr int WPB = BLK / 32;
     const int warp = threadIdx.x >> 5;
@@ -1842,16 +1928,18 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
             // next untaken group (groups cost unequal time: contacts, hits)
             if (threadIdx.x == 0) s_next[(st + 1) & 1] = g0 + WPB;  // last used by the previous step
             for (int wg = g0 + warp; wg < g1;) {
-                forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage, par, sim0, tab, cached,
-                                                                             &bl.rebuild, lone ? &bl : nullptr);
+                forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED, USER>(d, wg, stage, par, sim0, tab,
+                                                                                   cached, &bl.rebuild,
+                                                                                   lone ? &bl : nullptr);
                 int nx = 0;
                 if ((threadIdx.x & 31) == 0) nx = atomicAdd(&s_next[st & 1], 1);
                 wg = __shfl_sync(0xffffffffu, nx, 0);
             }
         } else {
             for (int wg = g0 + warp; wg < g1; wg += WPB)
-                forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED>(d, wg, stage, par, sim0, tab, cached,
-                                                                             &bl.rebuild, lone ? &bl : nullptr);
+                forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED, USER>(d, wg, stage, par, sim0, tab,
+                                                                                   cached, &bl.rebuild,
+                                                                                   lone ? &bl : nullptr);
         }
         if (SPLIT) {
             if (!grid_barrier(d.sync, bl, [](unsigned) { return -1; })) return;
@@ -1887,7 +1975,7 @@ __global__ void k_barrier_selftest(GridSync* gs) {
 
 // compute_gradients! (src/simulation.jl:150-158): forces and every gradient
 // buffer of the current state, no update.
-template <class T, int L, int S, bool ONE>
+template <class T, int L, int S, bool ONE, bool USER = false>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_gradients(DevPtrs<T> d, int par) {
     const int wpb = blockDim.x >> 5;
     const int wg = blockIdx.x * wpb + (threadIdx.x >> 5);
@@ -1896,7 +1984,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_gradients(DevPt
     const T* tab = stage_basis<T, ONE>(d);
     const SimDesc<T>* sim0 = copy_desc(d);
     int cached = -1;
-    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG>(d, wg, stage, par, sim0, tab, cached, nullptr, nullptr);
+    if (wg < ngroups) forces_warp<T, L, S, ONE, MODE_DIAG, USER>(d, wg, stage, par, sim0, tab, cached, nullptr, nullptr);
 }
 
 // Stand-alone rebuild phases (update_neighbors!, and the stateless neighbour

@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/fcc.h"
+#include "../../include/fcc_user_terms.h"
 #include "fcc_kernels.cuh"
 
 #ifndef FCC_NVTX
@@ -263,10 +264,18 @@ fcc_status make_spec(const fcc_params* p, const fcc_bodies_host* b, SimSpec<T>& 
     }
     if (p->nterms < 0 || p->nterms > FCC_MAX_TERMS || (p->nterms > 0 && !p->terms))
         return fail(FCC_ERR_ARGUMENT, "energy terms must be BodyTerms, ContactTerms or BondTerms");
+    int nuser[3] = {0, 0, 0};
     for (int q = 0; q < p->nterms; ++q) {
         const fcc_term& ft = p->terms[q];
-        if (ft.kind < FCC_TENSION || ft.kind > FCC_HARMONIC_BOND)
+        if (ft.kind < FCC_TENSION || ft.kind > FCC_USER_BOND)
             return fail(FCC_ERR_ARGUMENT, "energy terms must be BodyTerms, ContactTerms or BondTerms");
+        if (ft.kind >= FCC_USER_BODY) {
+            const int k = ft.kind - FCC_USER_BODY;
+            const int have = k == 0 ? fcc_user::n_body : k == 1 ? fcc_user::n_contact : fcc_user::n_bond;
+            if (ft.user < 0 || ft.user >= have) return fail(FCC_ERR_ARGUMENT, "no compiled user term with this index");
+            if (++nuser[k] > MUT)
+                return fail(FCC_ERR_UNSUPPORTED, "at most " + std::to_string(MUT) + " user terms of each kind");
+        }
         if (ft.ntypes_on < 0 || ft.ntypes_on > FCC_MAX_TYPES) return fail(FCC_ERR_ARGUMENT, "OnTypes: bad type list");
         if (ft.kind == FCC_OVERLAP && (ft.nJ < 1 || ft.nJ > FCC_MAX_TYPES))
             return fail(FCC_ERR_DIMENSION, "coupling tables must be square and equal-sized");
@@ -328,7 +337,14 @@ fcc_status make_spec(const fcc_params* p, const fcc_bodies_host* b, SimSpec<T>& 
     s.invLy = T(1) / s.Ly;
     s.dt = (T)p->dt;
     s.skin = (T)p->skin;
-    s.crange = T(0);  // interaction_range of the built-in contact terms
+    // contact_range (src/energies/contact.jl:54): the largest interaction
+    // range of the contact terms, in T (0 for the built-in ones)
+    s.crange = T(0);
+    for (int q = 0; q < p->nterms; ++q)
+        if (p->terms[q].kind == FCC_USER_CONTACT)
+            s.crange = std::max(s.crange, fcc_user::contact_range<T>(p->terms[q].user, (T)p->terms[q].a,
+                                                                    (T)p->terms[q].b));
+    if (!(s.crange >= T(0))) return fail(FCC_ERR_ARGUMENT, "interaction ranges must be non-negative");
     s.nbrange = s.crange + s.skin;
     s.dphi = (T)(2 * PI / nth);
     R0_h.resize(N);
@@ -337,7 +353,7 @@ fcc_status make_spec(const fcc_params* p, const fcc_bodies_host* b, SimSpec<T>& 
         R0_h[i] = (T)b->R0[i];
         maxR0 = std::max(maxR0, (double)R0_h[i]);
     }
-    const double cutoff = 2 * maxR0 * (1 + SHAPE_BOUND) + 0.0 + p->skin;  // src/simulation.jl:90
+    const double cutoff = 2 * maxR0 * (1 + SHAPE_BOUND) + (double)s.crange + p->skin;  // src/simulation.jl:90
     {
         int64_t gx = 0, gy = 0;
         FCC_TRY(cell_grid_dims((double)s.Lx, (double)s.Ly, cutoff, &gx, &gy));
@@ -405,8 +421,29 @@ fcc_status make_spec(const fcc_params* p, const fcc_bodies_host* b, SimSpec<T>& 
     }
     s.nbt = 0;
     s.nbd = 0;
+    s.nub = s.nuc = s.nubd = 0;
     for (int q = 0; q < p->nterms; ++q) {
         const fcc_term& ft = p->terms[q];
+        if (ft.kind == FCC_USER_BODY) {
+            const int u = s.nub++;
+            s.ub_id[u] = ft.user;
+            s.ub_mask[u] = mask_of(ft);
+            s.ub_a[u] = (T)ft.a;
+            s.ub_b[u] = (T)ft.b;
+        } else if (ft.kind == FCC_USER_CONTACT) {
+            const int u = s.nuc++;
+            s.uc_id[u] = ft.user;
+            s.uc_mask[u] = mask_of(ft);
+            s.uc_a[u] = (T)ft.a;
+            s.uc_b[u] = (T)ft.b;
+            has_contact = true;
+        } else if (ft.kind == FCC_USER_BOND) {
+            const int u = s.nubd++;
+            s.ubd_id[u] = ft.user;
+            s.ubd_mask[u] = mask_of(ft);
+            s.ubd_a[u] = (T)ft.a;
+            s.ubd_b[u] = (T)ft.b;
+        }
         if (ft.kind == FCC_TENSION || ft.kind == FCC_PERIMETER_ELASTICITY) {
             const int u = s.nbt++;
             s.bt_kind[u] = ft.kind == FCC_TENSION ? BT_TENSION : BT_PERIMETER;
@@ -710,6 +747,7 @@ struct Engine final : EngineBase {
         has_contact = sp.has_contact;
         split = sp.split;
         desc = sp.desc;
+        user = desc.nub + desc.nuc + desc.nubd > 0;
         type_h = std::move(sp.type);
         parent_h = std::move(sp.parent);
         R0_h = std::move(sp.R0);
@@ -787,8 +825,16 @@ struct Engine final : EngineBase {
     size_t stage_bytes() const {
         return basis_table_bytes<T>() + (size_t)(var().blk / 32) * (sizeof(T) == 4 ? var().stage32 : var().stage64);
     }
-    void* step_kernel() const { return (sizeof(T) == 4 ? var().f32 : var().f64)(one_chunk(), split); }
+    // compiled user terms: the 8 x 5 / 256-thread kernels with the user-term code
+    bool user = false;
+    void* step_kernel() const {
+        if (user)
+            return split ? (void*)k_step<T, 8, 5, true, true, 256, (sizeof(T) == 4 ? 2 : 1), true>
+                         : (void*)k_step<T, 8, 5, true, false, 256, (sizeof(T) == 4 ? 2 : 1), true>;
+        return (sizeof(T) == 4 ? var().f32 : var().f64)(one_chunk(), split);
+    }
     void* grad_kernel() const {
+        if (user) return (void*)k_gradients<T, LANES, SLOTS, true, true>;
         return nth <= LANES * SLOTS ? (void*)k_gradients<T, LANES, SLOTS, true> : (void*)k_gradients<T, LANES, SLOTS, false>;
     }
 
@@ -810,6 +856,10 @@ struct Engine final : EngineBase {
     // 52.0 µs).
     fcc_status choose_variant() {
         variant = 0;
+        if (user) {  // one kernel family carries the user-term code
+            if (!one_chunk()) return fail(FCC_ERR_UNSUPPORTED, "user terms need ntheta <= 40 (one contour chunk)");
+            return FCC_OK;
+        }
         if (const char* e = std::getenv("FCC_VARIANT")) {
             const int v = std::atoi(e);
             if (v >= 0 && v < NVARIANTS && (sizeof(T) == 4 || VARIANTS[v].f64)) variant = v;
@@ -1066,7 +1116,9 @@ struct Engine final : EngineBase {
         const DevPtrs<T> d = ptrs();
         const int64_t groups = (N + (32 / LANES) - 1) / (32 / LANES);
         const int grid = (int)((groups + 256 / 32 - 1) / (256 / 32));
-        if (nth <= LANES * SLOTS)
+        if (user)
+            k_gradients<T, LANES, SLOTS, true, true><<<grid, 256, grad_stage_bytes(), stream>>>(d, par());
+        else if (nth <= LANES * SLOTS)
             k_gradients<T, LANES, SLOTS, true><<<grid, 256, grad_stage_bytes(), stream>>>(d, par());
         else
             k_gradients<T, LANES, SLOTS, false><<<grid, 256, grad_stage_bytes(), stream>>>(d, par());

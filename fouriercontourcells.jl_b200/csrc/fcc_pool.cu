@@ -425,6 +425,8 @@ struct Pool final : PoolBase {
             return fail(FCC_ERR_ARGUMENT, "pool: x, y, theta and coef are required");
         SimSpec<T> sp;
         FCC_TRY(make_spec(p, b, sp));
+        if (sp.desc.nub + sp.desc.nuc + sp.desc.nubd > 0)
+            return fail(FCC_ERR_UNSUPPORTED, "pool: simulations with compiled user terms run alone (fcc_create)");
         if (sp.ccap > ccap || sp.bcap > bcap)
             return fail(FCC_ERR_UNSUPPORTED, "pool: more children or bonds per body than the pool was made for");
         FCC_TRY(compact());

@@ -179,6 +179,87 @@ class HarmonicBond(BondTerm):
         object.__setattr__(self, "r0", float(r0))
 
 
+class UserTerm(EnergyTerm):
+    """A user-defined term compiled into the library (include/fcc_user_terms.h):
+    the C++ functor at ``index`` of its kind's table, with parameters ``a``,
+    ``b``.  The reference's user terms are Julia structs with methods
+    (src/energies/interface.jl:27-106); here they are C++ functors, since a
+    Julia closure cannot cross the C ABI."""
+
+    index = 0
+
+    def __init__(self, a=0.0, b=0.0, index=None):
+        self.a, self.b = float(a), float(b)
+        if index is not None:
+            self.index = int(index)
+
+    def __eq__(self, other):
+        return type(self) is type(other) and (self.index, self.a, self.b) == (other.index, other.a, other.b)
+
+    def __hash__(self):
+        return hash((type(self).__name__, self.index, self.a, self.b))
+
+    def __repr__(self):
+        return f"{type(self).__name__}(a={self.a}, b={self.b}, index={self.index})"
+
+
+class UserBodyTerm(UserTerm, BodyTerm):
+    """A compiled user BodyTerm: E = F(Q), Q_j = ∮ q_j(R, R', R'') dφ."""
+
+    kind = 6
+
+
+class UserContactTerm(UserTerm, ContactTerm):
+    """A compiled user ContactTerm: energy density g(d) with an interaction range."""
+
+    kind = 7
+
+
+class UserBondTerm(UserTerm, BondTerm):
+    """A compiled user BondTerm: bond energy gradient dE/dΔ."""
+
+    kind = 8
+
+
+class Bending(UserBodyTerm):
+    """κ ∮ c² ds, the reference README's user-term example (README.md:118-121);
+    entry 0 of the compiled body terms."""
+
+    index = 0
+
+    def __init__(self, κ):
+        super().__init__(κ, 0.0)
+
+
+class ShapeIndexElasticity(UserBodyTerm):
+    """k (P / √A - p0)² of the perimeter P and area A (two integrals); entry 1
+    of the compiled body terms."""
+
+    index = 1
+
+    def __init__(self, k, p0):
+        super().__init__(k, p0)
+
+
+class Adhesion(UserContactTerm):
+    """Energy density -ε in a band of width w outside a neighbour's contour
+    (interaction range w); entry 0 of the compiled contact terms."""
+
+    index = 0
+
+    def __init__(self, ε, w):
+        super().__init__(ε, w)
+
+
+class QuarticBond(UserBondTerm):
+    """k |Δ|⁴ / 4 between bonded centres; entry 0 of the compiled bond terms."""
+
+    index = 0
+
+    def __init__(self, k):
+        super().__init__(k, 0.0)
+
+
 @dataclass(frozen=True)
 class OnTypes(EnergyTerm):
     """Restrict ``term`` to bodies whose type is in ``types``

@@ -56,13 +56,22 @@ enum {
     FCC_PERIMETER_ELASTICITY = 2,  /* PerimeterElasticity(l, p0): a = l, b = p0 */
     FCC_OVERLAP = 3,               /* Overlap(J; related):    J, Jrel tables     */
     FCC_LINEAR_REPULSION = 4,      /* LinearRepulsion(k):     a = k              */
-    FCC_HARMONIC_BOND = 5          /* HarmonicBond(k; r0):    a = k, b = r0      */
+    FCC_HARMONIC_BOND = 5,         /* HarmonicBond(k; r0):    a = k, b = r0      */
+    /* user terms compiled into the library (include/fcc_user_terms.h):
+     * fcc_term.user is the index in that kind's table, a and b its parameters */
+    FCC_USER_BODY = 6,             /* a BodyTerm: integrands q_j(R, R', R''), energy F(Q) */
+    FCC_USER_CONTACT = 7,          /* a ContactTerm: pressure g(d), interaction range    */
+    FCC_USER_BOND = 8              /* a BondTerm: bond energy gradient                   */
 };
 
 /* One energy term.  `ntypes_on > 0` wraps the term in OnTypes(term, types_on...)
  * (src/energies/interface.jl:278-298).  Overlap couplings are nJ x nJ tables,
  * column-major, indexed (type_i, type_j) like the reference's SMatrix
- * (src/energies/contact.jl:12-28); a scalar coupling is nJ = 1. */
+ * (src/energies/contact.jl:12-28); a scalar coupling is nJ = 1.  `user`
+ * selects the compiled user term of an FCC_USER_* kind (the reference's
+ * user-defined BodyTerm / ContactTerm / BondTerm, src/energies/interface.jl:27-106);
+ * at most FCC_MAX_USER_TERMS of each user kind per simulation. */
+#define FCC_MAX_USER_TERMS 4
 typedef struct {
     int32_t kind;
     int32_t ntypes_on;
@@ -71,6 +80,7 @@ typedef struct {
     int32_t nJ;
     double J[FCC_MAX_TYPES * FCC_MAX_TYPES];
     double Jrel[FCC_MAX_TYPES * FCC_MAX_TYPES];
+    int32_t user;
 } fcc_term;
 
 /* BodyType(; v0, Dr, Dt, mu_r, mu_theta, mu_ab, drag) (src/bodies.jl:30-45);

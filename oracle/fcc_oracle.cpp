@@ -11,6 +11,7 @@
 // Bodies are data-parallel (OpenMP), as the KernelAbstractions CPU backend is.
 
 #include "fcc_oracle.h"
+#include "../include/fcc_user_terms.h"
 
 #include <algorithm>
 #include <cmath>
@@ -108,6 +109,7 @@ const double SHAPE_BOUND = std::sqrt(2.0 / 3.0);  // src/dynamics.jl:26
 // ---------------------------------------------------------------- terms ----
 template <class T> struct Term {
     int kind = 0;
+    int user = 0;  // FCC_USER_*: index in the compiled table (include/fcc_user_terms.h)
     std::vector<int32_t> types_on;  // OnTypes; empty = all types
     T a = 0, b = 0;
     int nJ = 1;
@@ -207,8 +209,14 @@ template <class T> struct Sim final : SimBase {
             const fcc_term& ft = p->terms[q];
             Term<T> tm;
             tm.kind = ft.kind;
-            if (ft.kind < FCC_TENSION || ft.kind > FCC_HARMONIC_BOND)
+            if (ft.kind < FCC_TENSION || ft.kind > FCC_USER_BOND)
                 return fail(FCC_ERR_ARGUMENT, "energy terms must be BodyTerms, ContactTerms or BondTerms");
+            tm.user = ft.user;
+            const int nuser = ft.kind == FCC_USER_BODY ? fcc_user::n_body
+                              : ft.kind == FCC_USER_CONTACT ? fcc_user::n_contact
+                              : ft.kind == FCC_USER_BOND ? fcc_user::n_bond : 1;
+            if (ft.kind >= FCC_USER_BODY && (ft.user < 0 || ft.user >= nuser))
+                return fail(FCC_ERR_ARGUMENT, "no compiled user term with this index");
             if (ft.ntypes_on < 0 || ft.ntypes_on > FCC_MAX_TYPES) return fail(FCC_ERR_ARGUMENT, "OnTypes: bad type list");
             for (int u = 0; u < ft.ntypes_on; ++u) tm.types_on.push_back(ft.types_on[u]);
             tm.a = (T)ft.a;
@@ -219,8 +227,10 @@ template <class T> struct Sim final : SimBase {
                 to_T(tm.J, ft.J, (size_t)ft.nJ * ft.nJ);
                 to_T(tm.Jrel, ft.Jrel, (size_t)ft.nJ * ft.nJ);
             }
-            if (ft.kind == FCC_TENSION || ft.kind == FCC_PERIMETER_ELASTICITY) body_terms.push_back(tm);
-            else if (ft.kind == FCC_OVERLAP || ft.kind == FCC_LINEAR_REPULSION) contact_terms.push_back(tm);
+            if (ft.kind == FCC_TENSION || ft.kind == FCC_PERIMETER_ELASTICITY || ft.kind == FCC_USER_BODY)
+                body_terms.push_back(tm);
+            else if (ft.kind == FCC_OVERLAP || ft.kind == FCC_LINEAR_REPULSION || ft.kind == FCC_USER_CONTACT)
+                contact_terms.push_back(tm);
             else bond_terms.push_back(tm);
         }
         N = b->n;
@@ -283,7 +293,12 @@ template <class T> struct Sim final : SimBase {
         // cutoff and CellList (src/simulation.jl:90-91, src/neighbors.jl:27-33), in Float64 as Julia promotes
         double maxR0 = 0;
         for (int64_t i = 0; i < N; ++i) maxR0 = std::max(maxR0, (double)R0[i]);
-        double range64 = 0;  // contact_range: interaction_range of the built-in terms is 0
+        // contact_range (src/energies/contact.jl:54): the largest interaction
+        // range of the contact terms (0 for the built-in ones), in T
+        double range64 = 0;
+        for (const Term<T>& tm : contact_terms)
+            if (tm.kind == FCC_USER_CONTACT)
+                range64 = std::max(range64, (double)fcc_user::contact_range<T>(tm.user, tm.a, tm.b));
         double cutoff = 2 * maxR0 * (1 + SHAPE_BOUND) + range64 + p->skin;
         auto ncells = [&](T L) { int64_t n = (int64_t)std::floor((double)L / cutoff); return (int32_t)(n >= 3 ? n : 1); };
         ncx = ncells(Lx);
@@ -571,9 +586,31 @@ template <class T> struct Sim final : SimBase {
         T* gd = &GD[(size_t)nth * i];
         T* gdd = &GDD[(size_t)nth * i];
         std::vector<T> energies(body_terms.size(), T(0));
+        const T* r2 = &ddR[(size_t)nth * i];
         for (size_t q = 0; q < body_terms.size(); ++q) {
             const Term<T>& tm = body_terms[q];
             if (!tm.applies(type[i])) continue;
+            if (tm.kind == FCC_USER_BODY) {  // src/gradients.jl:70-98 with the term's own q, F
+                const int M = fcc_user::body_M(tm.user);
+                T Q[fcc_user::MAX_M] = {}, qk[fcc_user::MAX_M], dF[fcc_user::MAX_M], dq[fcc_user::MAX_M][3];
+                for (int k = 0; k < nth; ++k) {
+                    fcc_user::body_q<T>(tm.user, r[k], r1[k], r2[k], tm.a, tm.b, qk);
+                    for (int j = 0; j < M; ++j) Q[j] += qk[j];
+                }
+                for (int j = 0; j < M; ++j) Q[j] *= dphi;
+                fcc_user::body_dF<T>(tm.user, Q, R0[i], type[i], tm.a, tm.b, dF);
+                for (int k = 0; k < nth; ++k) {
+                    fcc_user::body_dq<T>(tm.user, r[k], r1[k], r2[k], tm.a, tm.b, dq);
+                    for (int j = 0; j < M; ++j) {
+                        const T w = dF[j] * dphi;
+                        gr[k] += dq[j][0] * w;
+                        gd[k] += dq[j][1] * w;
+                        gdd[k] += dq[j][2] * w;
+                    }
+                }
+                energies[q] = fcc_user::body_F<T>(tm.user, Q, R0[i], type[i], tm.a, tm.b);
+                continue;
+            }
             T Q = std::sqrt(r[0] * r[0] + r1[0] * r1[0]);
             for (int k = 1; k < nth; ++k) Q += std::sqrt(r[k] * r[k] + r1[k] * r1[k]);
             Q *= dphi;
@@ -613,6 +650,8 @@ template <class T> struct Sim final : SimBase {
                     size_t ij = nJ == 1 ? 0 : (size_t)(ti - 1) + (size_t)nJ * (tj - 1);
                     T J = rel ? tm.Jrel[ij] : tm.J[ij];
                     g = d >= 0 ? J : T(0);
+                } else if (tm.kind == FCC_USER_CONTACT) {
+                    g = fcc_user::contact_g<T>(tm.user, d, ti, tj, rel, tm.a, tm.b);
                 } else {
                     g = d > 0 ? tm.a * d : T(0);
                 }
@@ -677,10 +716,14 @@ template <class T> struct Sim final : SimBase {
                 const Term<T>& tm = bond_terms[u];
                 T h0 = 0, h1 = 0;
                 if (tm.applies(type[i]) && tm.applies(type[j])) {
-                    T rr = std::sqrt(d0 * d0 + d1 * d1);
-                    T f = rr > 0 ? tm.a * (T(1) - tm.b / rr) : (tm.b == 0 ? tm.a : T(0));
-                    h0 = f * d0;
-                    h1 = f * d1;
+                    if (tm.kind == FCC_USER_BOND) {
+                        fcc_user::bond_grad<T>(tm.user, d0, d1, type[i], type[j], tm.a, tm.b, h0, h1);
+                    } else {
+                        T rr = std::sqrt(d0 * d0 + d1 * d1);
+                        T f = rr > 0 ? tm.a * (T(1) - tm.b / rr) : (tm.b == 0 ? tm.a : T(0));
+                        h0 = f * d0;
+                        h1 = f * d1;
+                    }
                 }
                 a0 = h0 + a0;
                 a1 = h1 + a1;

@@ -15,9 +15,9 @@ against the CPU oracle with a stated tolerance:
   2..6 (BodyType maxmode, against the oracle with the same limit; 30 noisy
   FP64 steps at rtol 1e-8 and equal rebuild counts, and the nuclei's modes
   7..10 exactly zero after an FP32 run);
-- the N = 65536 polydisperse monolayer (256 x 256): one evaluation of the
-  forces of a deformed FP32 state against the FP64 oracle at 1e-5, flips
-  excluded and counted.
+- the N = 65536 and 262144 polydisperse monolayers (256 x 256, 512 x 512):
+  one evaluation of the forces of a deformed FP32 state against the FP64
+  oracle at 1e-5, flips excluded and counted.
 
 A Heaviside flip is a contour node whose Overlap pressure g = J H(d) differs
 between the two evaluations by at least J/2: FP32 rounding of the depth d
@@ -147,9 +147,10 @@ def test_nuclei_one_step_fp64_matches_oracle(nuclei_state, drag):
     assert np.abs(bg.coef - bo.coef).max() <= 1e-12 * dc + 1e-15
 
 
-# ----------------------------------------------------------- N = 65536 FP32
-def test_n65536_fp32_forces_vs_oracle():
-    bodies, box = fcc.polydisperse_monolayer(256, 256, packing=0.95, maxmode=10, seed=1234)
+# ------------------------------------------------ N = 65536 and 262144 FP32
+@pytest.mark.parametrize("side", [256, 512])
+def test_large_fp32_forces_vs_oracle(side):
+    bodies, box = fcc.polydisperse_monolayer(side, side, packing=0.95, maxmode=10, seed=1234)
     kw = dict(types=(fcc.BodyType(v0=0.06, Dr=0.01, μab=0.1),),
               energies=(fcc.Tension(0.01), fcc.Overlap(1.0), fcc.PerimeterElasticity(0.1, 3.7)), dt=0.005, seed=1234)
     g = G(bodies, box, T=np.float32, **kw)
@@ -158,7 +159,7 @@ def test_n65536_fp32_forces_vs_oracle():
     g.set_state(state)
     g.refresh()
     o = O(state, box, T=np.float64, **kw).refresh()
-    assert state.n == 65536
+    assert state.n == side * side
     flip = flips(g, o)
     assert flip.mean() <= 0.01
     for f in FIELDS:

@@ -186,6 +186,8 @@ def brute_force_pressure(sim):
                     continue
                 if isinstance(t, (fcc.Overlap, fcc.LinearRepulsion)):
                     P[:, i] += [t.pressure(dd, b.type[i], b.type[j], b.parent[i] == b.parent[j]) for dd in d]
+                elif isinstance(t, fcc.Adhesion):  # the compiled functor's g(d), restated
+                    P[:, i] += [-t.a if -t.b < dd < 0 else 0.0 for dd in d]
     return P
 
 
@@ -421,3 +423,67 @@ def test_type_maxmode_equals_a_simulation_with_fewer_modes():
         oracle.OracleSimulation(b6, box, **kw(7))
     with pytest.raises(fcc.ArgumentError):
         fcc.BodyType(maxmode=-1)
+
+
+# ------------------------------------------------------- compiled user terms
+@pytest.mark.parametrize("term", [fcc.Bending(0.3), fcc.ShapeIndexElasticity(0.7, 3.9)], ids=["Bending", "ShapeIndexElasticity"])
+def test_user_body_term_fd_shape_gradient(term):
+    """A compiled user BodyTerm (include/fcc_user_terms.h) through the same
+    finite-difference check as the built-ins (test/test_energies.jl:73-85,
+    rtol 1e-6); Bending needs R'' and its pullback (GDD)."""
+    sim, coef = single_body((term,))
+    sim.refresh()
+    g = sim.grad
+    assert np.abs(g.GDD).max() > 0 if isinstance(term, fcc.Bending) else np.abs(g.GDD).max() == 0
+    assert np.allclose(g.gcoef[1:, 0], fd_shape_gradient(sim, coef), rtol=1e-6, atol=1e-9)
+    assert g.gx[0] == 0 and g.gy[0] == 0 and g.gθ[0] == 0
+
+
+def test_user_bending_of_a_circle():
+    """∮ c² ds of a circle of radius R0 is 2π / R0."""
+    coef = np.zeros((11, 1))
+    coef[0] = 1
+    sim = O(fcc.Bodies.new([1.0], [2.0], [0.4], coef, [1.3]), fcc.PeriodicBox(20.0, 20.0),
+            types=(fcc.BodyType(),), energies=(fcc.Bending(0.25),), nθ=64).refresh()
+    assert math.isclose(sim.body_energy(), 0.25 * 2 * math.pi / 1.3, rel_tol=1e-12)
+
+
+def test_user_contact_term_matches_brute_force_and_widens_the_lists():
+    """A compiled user ContactTerm with an interaction range (Adhesion): the
+    node pressures equal the O(N²) restatement, and the range widens the
+    neighbour lists (contact_range, src/energies/contact.jl:54)."""
+    bodies, box = jittered_monolayer()
+    terms = (fcc.Overlap(1.0), fcc.Adhesion(0.4, 0.15))
+    sim = O(bodies, box, types=(fcc.BodyType(),), energies=terms).refresh()
+    P = sim.grad.P
+    assert (P < 0).sum() > 20  # nodes in the adhesion band
+    assert np.allclose(P, brute_force_pressure(sim), rtol=1e-12, atol=1e-12)
+    plain = O(bodies, box, types=(fcc.BodyType(),), energies=terms[:1]).refresh()
+    assert sim.neighbors.count.sum() > plain.neighbors.count.sum()
+
+
+def test_user_contact_two_discs_attract():
+    """Two discs a little apart, inside the adhesion band: the energy falls as
+    they approach (gradient towards the other body)."""
+    g = two_body((fcc.Adhesion(1.0, 0.2),), d=2.1, nθ=400).grad
+    assert g.gx[0] < -1e-3 and g.gx[1] > 1e-3
+    assert abs(g.gy[0]) < 1e-9
+
+
+def test_user_bond_term_gradient():
+    """A compiled user BondTerm (QuarticBond): dE/dΔ = k |Δ|² Δ on each centre."""
+    coef = np.zeros((11, 2))
+    coef[0] = 1
+    bodies = fcc.Bodies.new([5.0, 6.3], [5.0, 5.4], [0.1, 0.2], coef, [1.0, 1.0])
+    sim = O(bodies, fcc.PeriodicBox(20.0, 20.0), types=(fcc.BodyType(),), energies=(fcc.QuarticBond(0.7),),
+            bonds=[(1, 2)]).refresh()
+    dx, dy = 5.0 - 6.3, 5.0 - 5.4
+    r2 = dx * dx + dy * dy
+    assert np.allclose([sim.grad.gx[0], sim.grad.gy[0]], [0.7 * r2 * dx, 0.7 * r2 * dy], rtol=1e-12)
+    assert np.allclose([sim.grad.gx[1], sim.grad.gy[1]], [-0.7 * r2 * dx, -0.7 * r2 * dy], rtol=1e-12)
+
+
+def test_unknown_user_term_is_an_argument_error():
+    sim_args = dict(types=(fcc.BodyType(),), energies=(fcc.UserBodyTerm(1.0, 0.0, index=99),))
+    with pytest.raises(fcc.ArgumentError):
+        single_body(sim_args["energies"])
