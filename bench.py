@@ -579,10 +579,15 @@ def gpu_arm(args):
         steps_per_launch = steps / max(1, launches)
         bytes_launch = bytes_b * N * steps_per_launch
         achieved_gbs = bytes_launch / (launch_ms * 1e-3) / 1e9
+        # DRAM bytes of one timed launch from the committed ncu capture of this
+        # launch shape (exact when its step count was captured, else the
+        # steady-state bytes per step scaled to the launch)
         traffic = None
         try:
             prof = json.load(open(PROFILE_SUMMARY))
-            traffic = prof["dram_bytes_per_step"] * steps_per_launch
+            by = prof.get("dram_bytes_per_launch_by_steps", {})
+            key = str(int(round(steps_per_launch)))
+            traffic = float(by[key]) if key in by else prof["dram_bytes_per_step"] * steps_per_launch
         except Exception:
             pass
         cs = clk.summary()
