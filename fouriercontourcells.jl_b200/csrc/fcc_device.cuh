@@ -371,10 +371,12 @@ struct NoAfter {
 };
 // `after(code)` runs in thread 0 of the last block right after the release
 // (writes that no block reads before the next barrier).
+// `tick` is added to bl.clock before the closing block barrier, so every warp
+// of the block leaves with the new clock (a lone simulation's noise counter).
 // LIMIT: polls before a waiting block gives up (a self-test lowers it).
 template <long long LIMIT = SPIN_LIMIT, class F, class A = NoAfter>
 __device__ __forceinline__ bool grid_barrier(GridSync* gs, BarrierLocal& bl, F&& last, unsigned bits = 0,
-                                             A&& after = A{}) {
+                                             A&& after = A{}, int tick = 0) {
     __shared__ int s_last, s_err;
     __shared__ unsigned s_bits;
     unsigned* cnt = ((bl.gen >> GEN_FLAG_BITS) & 1u) ? &gs->count2 : &gs->count;
@@ -419,6 +421,7 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, BarrierLocal& bl, F&&
     if (threadIdx.x == 0) {
         bl.any = (int)(bl.gen & 1u);
         bl.flags = (int)((bl.gen >> 1) & 0xffu);
+        bl.clock += tick;
     }
     __syncthreads();
     return s_err == 0;

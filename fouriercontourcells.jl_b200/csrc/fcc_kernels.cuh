@@ -1952,13 +1952,16 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
             rb = bl.rebuild ? 1u : 0u;
             bl.rebuild = 0;
         }
+        // a lone simulation that stepped ticks its block-local clock inside the
+        // barrier: the next step's warps read it for their noise
+        const int tick = (lone && (f0 & F_ACTIVE) && !(f0 & (F_FROZEN | F_HOLD))) ? 1 : 0;
         if (!grid_barrier(
                 d.sync, bl, [&](unsigned rbs) { return bookkeeping(d, bl, rbs, sim0); }, rb,
                 [&](int code) {
                     if (lone) lone_book_writes(d, bl, code);
-                }))
+                },
+                tick))
             return;
-        if (threadIdx.x == 0 && lone && (f0 & F_ACTIVE) && !(f0 & (F_FROZEN | F_HOLD))) bl.clock += 1;
     }
 }
 

@@ -66,6 +66,22 @@ def test_pool_equals_alone_bitwise(T):
     assert not np.array_equal(pool.bodies(slots[0]).x[:10], pool.bodies(slots[1]).x[:10])
 
 
+def test_long_lone_run_equals_pool_bitwise():
+    """A lone FP32 simulation of 10000 bodies over 20000 steps (40 launches of
+    512 steps, warps taking groups dynamically) repeats bit for bit and equals
+    its pool run: the block-local noise clock every warp reads is ticked
+    before the step's closing block barrier."""
+    bodies, box, kw = monolayer(100, 100, 21, v0=0.1, eta=0.01, perimeter=True)
+    steps = 20000
+    first, second = alone(bodies, box, kw, np.float32, steps), alone(bodies, box, kw, np.float32, steps)
+    pool = fcc.Pool(T=np.float32, max_bodies=16384, max_cells=16384, max_sims=2)
+    slot = pool.add(bodies, box, horizon=steps, **kw)
+    pool.run(steps)
+    for f in ("x", "y", "θ", "coef", "imgx", "imgy"):
+        assert np.array_equal(getattr(first.bodies, f), getattr(second.bodies, f)), f
+    assert_same(pool, slot, first)
+
+
 @pytest.mark.parametrize("variant", [0, 3])
 def test_pool_with_many_slots_takes_the_full_scan_rebuild(variant, monkeypatch):
     """A rebuild visits the bodies and cells of the rebuilding simulations
