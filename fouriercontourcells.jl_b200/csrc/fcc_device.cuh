@@ -342,6 +342,9 @@ struct BarrierLocal {
     int flags;        // one simulation: its flags as of the last barrier
     long long clock;  // one simulation: its clock, ticked by every block
     int rebuild;      // a body of this block exceeded its skin in this step
+    int released;     // this block arrived last and released the barrier itself
+    int err;          // this block's wait gave up
+    unsigned bits;    // arrival bits summed up to this block's arrival
 };
 
 // Generation word: bit 0 the released any_need flag, bits 1-8 the flags of a
@@ -358,38 +361,40 @@ __device__ __forceinline__ void barrier_start(GridSync* gs, BarrierLocal& bl, bo
         bl.flags = one ? ld_acquire(flags) : 0;
         bl.clock = one ? *(volatile const long long*)clock : 0;
         bl.rebuild = 0;
+        bl.released = 0;
+        bl.err = 0;
     }
     __syncthreads();
 }
 
-// Arrival carries `bits` (summed over blocks into the upper half of the
-// counter).  `last(sum_bits)` runs with all threads of the last block and
+// A grid barrier in two halves.  barrier_arrive: the block arrives; the
+// last block to arrive runs `last(sum_bits)` with all its threads, which
 // returns (in thread 0) the code to release — any_need | flags << 1 — or -1
-// to keep the current one.
+// to keep the current one, releases the barrier and runs `after(code)` in
+// thread 0 (writes that no block reads before the next barrier).  Arrival
+// carries `bits` (summed over blocks into the upper half of the counter).
+// `tick` is added to bl.clock (a lone simulation's noise counter) before the
+// closing block barrier, so every warp of the block leaves with the new
+// clock.  barrier_wait: the block waits for the release and takes the
+// released rebuild flag and lone-simulation flags.  Between the halves a
+// block may only do work that reads no other block's writes of the step.
 struct NoAfter {
     __device__ void operator()(int) const {}
 };
-// `after(code)` runs in thread 0 of the last block right after the release
-// (writes that no block reads before the next barrier).
-// `tick` is added to bl.clock before the closing block barrier, so every warp
-// of the block leaves with the new clock (a lone simulation's noise counter).
-// LIMIT: polls before a waiting block gives up (a self-test lowers it).
-template <long long LIMIT = SPIN_LIMIT, class F, class A = NoAfter>
-__device__ __forceinline__ bool grid_barrier(GridSync* gs, BarrierLocal& bl, F&& last, unsigned bits = 0,
-                                             A&& after = A{}, int tick = 0) {
-    __shared__ int s_last, s_err;
-    __shared__ unsigned s_bits;
+template <class F, class A = NoAfter>
+__device__ __forceinline__ void barrier_arrive(GridSync* gs, BarrierLocal& bl, F&& last, unsigned bits = 0,
+                                               A&& after = A{}, int tick = 0) {
     unsigned* cnt = ((bl.gen >> GEN_FLAG_BITS) & 1u) ? &gs->count2 : &gs->count;
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned prev = atom_add_acq_rel(cnt, 1u + (bits << 16));
-        s_last = ((prev & 0xffffu) == gridDim.x - 1);
-        s_bits = (prev >> 16) + bits;
-        s_err = 0;
+        bl.released = ((prev & 0xffffu) == gridDim.x - 1);
+        bl.bits = (prev >> 16) + bits;
+        bl.err = 0;
     }
     __syncthreads();
-    if (s_last) {
-        int code = last(s_bits);
+    if (bl.released) {
+        int code = last(bl.bits);
         __syncthreads();
         if (threadIdx.x == 0) {
             if (code < 0) code = bl.any | (bl.flags << 1);
@@ -403,28 +408,43 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, BarrierLocal& bl, F&&
             after(code);
             bl.gen = ng;
         }
-    } else if (threadIdx.x == 0) {
-        long long it = 0;
-        unsigned v;
-        while ((v = ld_acquire(&gs->gen)) == bl.gen) {
-            if (++it > LIMIT) {
-                atomicExch(&gs->error, 1);
-                s_err = 1;
-                break;
-            }
-#if FCC_BARRIER_SLEEP > 0
-            __nanosleep(FCC_BARRIER_SLEEP);
-#endif
-        }
-        bl.gen = v;
     }
+    if (threadIdx.x == 0) bl.clock += tick;
+    __syncthreads();
+}
+
+// LIMIT: polls before a waiting block gives up (a self-test lowers it).
+template <long long LIMIT = SPIN_LIMIT>
+__device__ __forceinline__ bool barrier_wait(GridSync* gs, BarrierLocal& bl) {
     if (threadIdx.x == 0) {
+        if (!bl.released) {
+            long long it = 0;
+            unsigned v;
+            while ((v = ld_acquire(&gs->gen)) == bl.gen) {
+                if (++it > LIMIT) {
+                    atomicExch(&gs->error, 1);
+                    bl.err = 1;
+                    break;
+                }
+#if FCC_BARRIER_SLEEP > 0
+                __nanosleep(FCC_BARRIER_SLEEP);
+#endif
+            }
+            bl.gen = v;
+        }
         bl.any = (int)(bl.gen & 1u);
         bl.flags = (int)((bl.gen >> 1) & 0xffu);
-        bl.clock += tick;
     }
     __syncthreads();
-    return s_err == 0;
+    return bl.err == 0;
+}
+
+// Both halves, nothing between them.
+template <long long LIMIT = SPIN_LIMIT, class F, class A = NoAfter>
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, BarrierLocal& bl, F&& last, unsigned bits = 0,
+                                             A&& after = A{}, int tick = 0) {
+    barrier_arrive(gs, bl, static_cast<F&&>(last), bits, static_cast<A&&>(after), tick);
+    return barrier_wait<LIMIT>(gs, bl);
 }
 
 // Fast reciprocal square root for the FP32 force path (rsqrt, ~2 ulp);
