@@ -661,12 +661,6 @@ constexpr int NBMAX = 12;
 #ifndef FCC_DYN
 #define FCC_DYN 1  // 1: FP32, one simulation: warps take their block's warp groups dynamically
 #endif
-#ifndef FCC_BARRIER_OVERLAP
-// 1: a lone single-chunk simulation overlaps each step's closing barrier with
-// the next step's own-body work (measured: 16384 bodies 25.99 vs 26.16 us per
-// step, 65536 bodies 88.6 vs 85.3 us, 1024 bodies 10.91 vs 11.04 us: off)
-#define FCC_BARRIER_OVERLAP 0
-#endif
 
 // FP32 single-chunk kernels read cos(n phi_k), sin(n phi_k) (and n times
 // them) of their contour nodes from a shared-memory table instead of running
@@ -1151,18 +1145,9 @@ enum : int { MODE_FUSED = 0, MODE_FORCES = 1, MODE_DIAG = 2 };
 // USER: the simulation has compiled user terms (include/fcc_user_terms.h):
 // R'' is synthesised, user integrals, node gradients (GDD included),
 // pressures and bond gradients are added, and the pullback includes R''.
-// `defer` (a lone simulation, the first warp group of each warp in a step
-// whose opening barrier is still outstanding): the own-body part — own record,
-// Philox, synthesis, contour integrals — runs with the flags and ticked clock
-// the block already holds; then the block waits for the release
-// (barrier_wait, every warp of the block once) and only then stages the
-// neighbour records, which other blocks wrote in the previous step.  If the
-// release asks for a list rebuild (or the wait gave up) the warp returns
-// with nothing written, and the caller redoes the group after the rebuild.
 template <class T, int L, int S, bool ONE, int MODE, bool USER = false>
 __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stage, int par, const SimDesc<T>* sim0,
-                                            const T* tab, int& cached, int* rbp, BarrierLocal* lone,
-                                            GridSync* defer = nullptr) {
+                                            const T* tab, int& cached, int* rbp, const BarrierLocal* lone) {
     constexpr int BPW = 32 / L;
     constexpr unsigned FULL = 0xffffffffu;
     constexpr int CH16 = RECW * (int)sizeof(T) / 16;  // 16-byte chunks per record
@@ -1255,7 +1240,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
         }
         cp_async_commit();
     };
-    if (!defer) stage_batch(0);
+    stage_batch(0);
     int staged_base = 0;
 
     const int wv = unpack_w(wf);
@@ -1333,10 +1318,7 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
             if (!(vmask & (1u << sl))) R[sl] = R1[sl] = R2[sl] = T(0);
     };
 
-    if (defer)
-        cp_async_wait_all();  // the own record: the only copy in flight
-    else
-        cp_async_wait_group<1>();  // the own record (the neighbour copies may still fly)
+    cp_async_wait_group<1>();  // the own record (the neighbour copies may still fly)
     __syncwarp();
     // ---- pass 1: contour integral Q = sum_k sqrt(R^2 + R'^2) dphi
     T Qp = T(0);
@@ -1371,12 +1353,6 @@ __device__ __forceinline__ void forces_warp(const DevPtrs<T>& d, int wg, T* stag
 #pragma unroll
             for (int j = 0; j < fcc_user::MAX_M; ++j) UQ[u][j] = group_sum<L>(UQ[u][j]) * dphi;
         }
-    }
-
-    if (defer) {
-        // the previous step's release: the neighbours' records of this step are written
-        if (!barrier_wait(defer, *lone) || lone->any) return;
-        stage_batch(0);
     }
 
     // ---- body terms: W = sum_t dF_t/dQ * dphi, E = e_1 + (e_2 + ...)
@@ -1973,67 +1949,37 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
     __shared__ int s_next[2];  // next untaken warp group of the block, per step parity
     if (dyn && threadIdx.x == 0) s_next[0] = g0 + WPB;
     __syncthreads();
-    // A lone simulation of one contour chunk without the parent-drag split
-    // overlaps each step's closing barrier with the next step's own-body
-    // work: the blocks arrive, every warp runs the own-body part of its first
-    // warp group, and waits for the release inside it (forces_warp `defer`);
-    // the last step's release is not waited for (the launch's end orders it
-    // before the host's reads).  Multi-chunk kernels keep the plain barrier
-    // (the deferred path adds spills there).
-    constexpr bool OVL = FCC_BARRIER_OVERLAP && ONE && !SPLIT;
-    const bool overlap = OVL && lone;
-    bool pending = false;  // the previous step's closing barrier is not yet waited for
     for (int st = 0; st < nsteps; ++st) {
         const int par = (par0 + st) & 1;
-        // the block's next untaken group of the next step (this slot was last used
-        // in the previous step, which every warp has left)
-        if (dyn && threadIdx.x == 0) s_next[(st + 1) & 1] = g0 + WPB;
-        // A warp's first group is its own; after that it takes the block's next
-        // untaken group (one FP32 simulation: groups cost unequal time — contacts,
-        // hits) or the next of its static share.  One call site each of the
-        // rebuild and of forces_warp, so that every launch shape and path runs
-        // the same compiled arithmetic.
-        bool rebuild = !(OVL && pending) && bl.any;
-        int wg = g0 + warp;
-        for (;;) {
-            if (rebuild) {
-                // the work list of a pool lives in the warps' stage area, free
-                // between the closing barrier of a step and the forces
-                if (!rebuild_prologue(d, par, tid, nthr, bl, sim0, reinterpret_cast<int*>(block_stage_of<T>()),
-                                      (int)(WPB * stage_bytes_per_warp<T, L>() / sizeof(int))))
-                    return;
-                cached = -1;  // the descriptor slots were overwritten
-                rebuild = false;
-            }
-            const bool deferred = OVL && pending;  // only a warp's first group
-            if (wg < g1)
-                forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED, USER>(
-                    d, wg, stage, par, sim0, tab, cached, &bl.rebuild, lone ? &bl : nullptr,
-                    deferred ? d.sync : nullptr);
-            else if (deferred)
-                barrier_wait(d.sync, bl);
-            if (deferred) {
-                pending = false;
-                if (bl.err) return;
-                if (bl.any) {
-                    // the release asks for a list rebuild: the first groups' own-body
-                    // work is discarded and done again on the new lists
-                    rebuild = true;
-                    continue;
-                }
-            }
-            if (wg >= g1) break;
-            if (dyn) {
+        if (bl.any) {
+            // the work list of a pool lives in the warps' stage area, free
+            // between the closing barrier of a step and the forces
+            if (!rebuild_prologue(d, par, tid, nthr, bl, sim0, reinterpret_cast<int*>(block_stage_of<T>()),
+                                  (int)(WPB * stage_bytes_per_warp<T, L>() / sizeof(int))))
+                return;
+            cached = -1;  // the descriptor slots were overwritten
+        }
+        if (dyn) {
+            // a warp's first group is its own; after that it takes the block's
+            // next untaken group (groups cost unequal time: contacts, hits)
+            if (threadIdx.x == 0) s_next[(st + 1) & 1] = g0 + WPB;  // last used by the previous step
+            for (int wg = g0 + warp; wg < g1;) {
+                forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED, USER>(d, wg, stage, par, sim0, tab,
+                                                                                   cached, &bl.rebuild,
+                                                                                   lone ? &bl : nullptr);
                 int nx = 0;
                 if ((threadIdx.x & 31) == 0) nx = atomicAdd(&s_next[st & 1], 1);
                 wg = __shfl_sync(0xffffffffu, nx, 0);
-            } else {
-                wg += WPB;
             }
+        } else {
+            for (int wg = g0 + warp; wg < g1; wg += WPB)
+                forces_warp<T, L, S, ONE, SPLIT ? MODE_FORCES : MODE_FUSED, USER>(d, wg, stage, par, sim0, tab,
+                                                                                   cached, &bl.rebuild,
+                                                                                   lone ? &bl : nullptr);
         }
         if (SPLIT) {
             if (!grid_barrier(d.sync, bl, [](unsigned) { return -1; })) return;
-            for (int wu = g0 + warp; wu < g1; wu += WPB) update_warp_split<T, L>(d, wu, par, sim0, &bl.rebuild);
+            for (int wg = g0 + warp; wg < g1; wg += WPB) update_warp_split<T, L>(d, wg, par, sim0, &bl.rebuild);
         }
         __syncthreads();  // every warp's skin verdict is in bl.rebuild
         const int f0 = bl.flags;
@@ -2045,17 +1991,13 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
         // a lone simulation that stepped ticks its block-local clock inside the
         // barrier: the next step's warps read it for their noise
         const int tick = (lone && (f0 & F_ACTIVE) && !(f0 & (F_FROZEN | F_HOLD))) ? 1 : 0;
-        barrier_arrive(
-            d.sync, bl, [&](unsigned rbs) { return bookkeeping(d, bl, rbs, sim0); }, rb,
-            [&](int code) {
-                if (lone) lone_book_writes(d, bl, code);
-            },
-            tick);
-        if (overlap) {
-            pending = st + 1 < nsteps;
-        } else if (!barrier_wait(d.sync, bl)) {
+        if (!grid_barrier(
+                d.sync, bl, [&](unsigned rbs) { return bookkeeping(d, bl, rbs, sim0); }, rb,
+                [&](int code) {
+                    if (lone) lone_book_writes(d, bl, code);
+                },
+                tick))
             return;
-        }
     }
 }
 
