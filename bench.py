@@ -415,10 +415,13 @@ def trajectory_audit(fcc, oracle, r, steps=AUDIT_STEPS):
             "pass": bool(within >= 0.95 and (dr <= bound_dr).all() and (dc <= bound_dc).all())}
 
 
-def serving_leg(fcc, oracle, work=1.5e10, pool_bodies=1 << 18, policy="fifo"):
+def serving_leg(fcc, oracle, work=1.5e10, pool_bodies=1 << 18, policy="fifo", plain=True, check_every=1):
     """The first requests of the serving stream (up to `work` body-steps),
     served by continuous batching on one pool sized from an HBM budget, then
-    the same requests run one at a time (the plain loop)."""
+    the same requests run one at a time (the plain loop), each result
+    compared bit for bit with the served one.  `plain` False (the whole
+    stream): no plain loop; every `check_every`-th request is run alone for
+    the bitwise comparison only."""
     import torch
     stream = serve_stream()
     offered = 20.0 * float(np.mean([sp["nx"] * sp["ny"] * sp["horizon"] for sp in stream]))
@@ -439,7 +442,8 @@ def serving_leg(fcc, oracle, work=1.5e10, pool_bodies=1 << 18, policy="fifo"):
     by_id = {r.id: r for r in res}
     # the plain loop: each request alone, in arrival order
     durations, equal = [], 0
-    for r in reqs:
+    solo = reqs if plain else reqs[::check_every]
+    for r in solo:
         t0 = time.perf_counter()
         sim = fcc.Simulation(r.bodies, r.box, T=np.float32, **r.kw)
         sim.run(r.horizon)
@@ -448,10 +452,12 @@ def serving_leg(fcc, oracle, work=1.5e10, pool_bodies=1 << 18, policy="fifo"):
         c = by_id[r.id].bodies
         equal += int(all(np.array_equal(getattr(b, f), getattr(c, f)) for f in ("x", "y", "θ", "coef", "imgx")))
         sim.close()
-    lat = fcc.serving.sequential_latencies([r.arrival for r in reqs], durations)
-    plain_span = max(a + l for a, l in zip((r.arrival for r in reqs), lat)) - min(r.arrival for r in reqs)
-    plain = {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-             "body_steps_per_s": served["body_steps"] / plain_span}
+    plain_stats = None
+    if plain:
+        lat = fcc.serving.sequential_latencies([r.arrival for r in reqs], durations)
+        plain_span = max(a + l for a, l in zip((r.arrival for r in reqs), lat)) - min(r.arrival for r in reqs)
+        plain_stats = {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                       "body_steps_per_s": served["body_steps"] / plain_span}
     # audited requests: at least 20 (or all), spread over the sample; each
     # served result equals its solo run bit for bit (checked above for every
     # request), so the audit checks that solo path against the FP64 oracle:
@@ -467,10 +473,10 @@ def serving_leg(fcc, oracle, work=1.5e10, pool_bodies=1 << 18, policy="fifo"):
             "sample": f"the first {len(reqs)} requests of the seeded 2000-request stream ({acc:.3g} body-steps)",
             "offered_body_steps_per_s": offered,
             "pool": {"hbm_budget_bytes": budget, "max_bodies": u["max_bodies"], "max_sims": u["max_sims"]},
-            "policy": policy, "served": served, "plain": plain,
-            "served_over_plain": served["body_steps_per_s"] / plain["body_steps_per_s"],
+            "policy": policy, "served": served, "plain": plain_stats,
+            "served_over_plain": served["body_steps_per_s"] / plain_stats["body_steps_per_s"] if plain else None,
             "chunks": srv.chunks, "device_busy_fraction": srv.device_ms * 1e-3 / max(served["makespan_s"], 1e-9),
-            "bitwise_equal_to_alone": f"{equal}/{len(reqs)}",
+            "bitwise_equal_to_alone": f"{equal}/{len(solo)}",
             "audited": len(audit),
             "audit_force_error_vs_fp64": errs,
             "audit_trajectory_vs_fp64": {
@@ -710,6 +716,10 @@ def main():
     ap.add_argument("--serve-policy", default="fifo", choices=["fifo", "sjf"], help="serving admission order")
     ap.add_argument("--serve-pool-bodies", type=int, default=1 << 18,
                     help="bodies the serving pool's HBM budget is sized for")
+    ap.add_argument("--serve-no-plain", action="store_true",
+                    help="serving leg without the plain loop (the whole stream); see --serve-check-every")
+    ap.add_argument("--serve-check-every", type=int, default=1,
+                    help="with --serve-no-plain: every k-th request is run alone for the bitwise comparison")
     ap.add_argument("--only", choices=["batched", "serving"],
                     help="run one leg alone and print its JSON (profiling; not the bench line)")
     args = ap.parse_args()
@@ -721,7 +731,8 @@ def main():
         fcc = load_package()
         out = batched_leg(fcc, steps=args.batch_steps) if args.only == "batched" else \
             serving_leg(fcc, load_oracle(), work=args.serve_work, policy=args.serve_policy,
-                        pool_bodies=args.serve_pool_bodies)
+                        pool_bodies=args.serve_pool_bodies, plain=not args.serve_no_plain,
+                        check_every=max(1, args.serve_check_every))
         print(json.dumps({"leg": args.only, **out}, default=str), flush=True)
     else:
         gpu_arm(args)
