@@ -98,6 +98,7 @@ class NativeSimulation:
         self._fn = lambda name: getattr(self._lib, self._pfx + name)
         self._params = abi.ParamsBuffer(box, types, energies, bonds, dt, nθ, T, seed, skin, nl_capacity)
         self._buf = None  # host arrays in the ABI's layout, reused for inputs that are not
+        self._direct = {}  # writable -> (bodies, its arrays, fcc_bodies_host over them)
         h = C.c_void_p()
         self._call("create", C.byref(self._params.p), C.byref(self._host_in(bodies)), C.byref(h))
         self._h = h
@@ -116,6 +117,7 @@ class NativeSimulation:
         abi.check(self._fn(name)(*args), self._lib._lasterr)
 
     def close(self):
+        self._direct = {}
         if getattr(self, "_h", None):
             self._fn("destroy")(self._h)
             self._h = None
@@ -149,10 +151,28 @@ class NativeSimulation:
         return self.compute_gradients()
 
     # ---------------------------------------------------------------- state
+    _FIELDS = ("x", "y", "θ", "imgx", "imgy", "coef", "R0", "type", "parent")
+
+    def _direct_host(self, bodies: Bodies, writable: bool = False):
+        """``abi.direct_host(bodies)``, kept for the next call with the same
+        ``Bodies`` holding the same array objects (the exchange loop of a
+        caller that reuses its page-locked buffers): the check is nine
+        identity tests instead of nine layout checks.  The entry holds
+        references to the arrays, so none of them is freed (and its address
+        reused) while the kept pointers refer to it."""
+        c = getattr(self, "_direct", {}).get(writable)
+        if (c is not None and c[0] is bodies and all(getattr(bodies, f) is a for f, a in zip(self._FIELDS, c[1]))
+                and (not writable or all(a.flags.writeable for a in c[1]))):
+            return c[2]
+        h = abi.direct_host(bodies, writable=writable)
+        if h is not None and hasattr(self, "_direct"):
+            self._direct[writable] = (bodies, tuple(getattr(bodies, f) for f in self._FIELDS), h)
+        return h
+
     def _host_in(self, bodies: Bodies):
         """An ``fcc_bodies_host`` over `bodies` itself when its arrays are in
         the ABI's layout, else over a copy in a buffer this object keeps."""
-        h = abi.direct_host(bodies)
+        h = self._direct_host(bodies)
         if h is not None:
             return h
         if self._buf is None or self._buf.n != bodies.n or self._buf.ncoef != bodies.ncoef:
@@ -171,7 +191,7 @@ class NativeSimulation:
         device-to-host copy per array when they are in the ABI's layout, a DMA
         when `out` is ``pinned_bodies``), else into new arrays."""
         if out is not None:
-            h = abi.direct_host(out, writable=True)
+            h = self._direct_host(out, writable=True)
             if h is None or out.n != self.N or out.ncoef != self.ncoef:
                 raise ArgumentError("get_state(out=...) needs writable arrays of this simulation's size in the "
                                     "ABI's layout (contiguous vectors, coef in Fortran order): see pinned_bodies")
