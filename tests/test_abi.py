@@ -175,3 +175,33 @@ def test_ctypes_signatures_match_the_header():
         assert [_ctypes_kind(a) for a in args] == [_header_kind(p) for p in params], name
         checked += 1
     assert checked >= 30
+
+
+def test_host_exchange_struct_is_kept_for_the_same_arrays():
+    """set_state / get_state(out) keep the exchange struct of the last Bodies
+    passed (the same marshalling serves the oracle): reused while the object
+    holds the same arrays, rebuilt when an array is replaced, dropped by
+    close(); the exchanged values are the same either way."""
+    bodies, box = fcc.hexagonal_monolayer(4, 4, packing=0.9, maxmode=6, rng=3)
+    kw = dict(types=(fcc.BodyType(v0=0.1, Dr=0.01),), energies=(fcc.Tension(0.1), fcc.Overlap(1.0)), T=np.float64)
+    sim = oracle.OracleSimulation(bodies, box, **kw)
+    state = sim.bodies
+    state.coef = np.asfortranarray(state.coef)
+    h1 = sim._direct_host(state)
+    assert h1 is not None and sim._direct_host(state) is h1
+    state.x = state.x.copy()  # a replaced array: a new struct over it
+    h2 = sim._direct_host(state)
+    assert h2 is not h1 and C.cast(h2.x, C.c_void_p).value == state.x.ctypes.data
+    sim.set_state(state)
+    out = sim.bodies
+    out.coef = np.asfortranarray(out.coef)
+    sim.get_state(out=out)
+    assert np.array_equal(out.x, state.x) and np.array_equal(out.coef, state.coef)
+    ro = out.copy()
+    ro.coef = np.asfortranarray(ro.coef)
+    sim.get_state(out=ro)
+    ro.x.flags.writeable = False  # no longer writable: the kept struct is not used
+    with pytest.raises(fcc.ArgumentError):
+        sim.get_state(out=ro)
+    sim.close()
+    assert sim._direct == {}
