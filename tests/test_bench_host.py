@@ -51,3 +51,57 @@ def test_force_error_excludes_only_heaviside_flips():
     err = bench.force_error(OracleFP32, oracle, o.bodies, box, kw)
     assert err["max_rel"] < 1e-5, err
     assert 1 <= err["excluded_flips"] and err["excluded_fraction"] < 0.01, err  # this state holds one flip
+
+
+def _request(bench, side=16):
+    sp = dict(bench.serve_stream()[3])
+    sp.update(nx=side, ny=side)
+    return bench.make_request(fcc, sp)
+
+
+def test_trajectory_audit_passes_fp32_against_fp64():
+    """The serving audit's replay with the FP32 oracle standing in for the
+    CUDA path: every body within its flip-charged bound."""
+    bench = load_bench()
+    res = bench.trajectory_audit(OracleFP32, oracle, _request(bench))
+    assert res["pass"] and res["frac_within"] >= 0.95, res
+    assert res["max_dr_over_bound"] <= 1.0 and res["max_dcoef_over_bound"] <= 1.0, res
+
+
+def test_trajectory_audit_charges_a_flip_to_the_two_ring():
+    """A flip planted in the probe's pressures at one node of body 101, every
+    step: counted once per step, charged to that body, its list neighbours
+    and theirs, and to no one else."""
+    bench = load_bench()
+    made = []
+
+    class Planted(oracle.OracleSimulation):
+        @property
+        def grad(self):
+            gr = super().grad
+            if self is made[1]:  # the audit's second simulation is its probe
+                P = np.array(gr.P)
+                P[3, 100] += 1.0
+                gr = gr._replace(P=P)
+            return gr
+
+    class NS:
+        Overlap = fcc.Overlap
+
+        @staticmethod
+        def Simulation(bodies, box, T, **kw):
+            made.append(Planted(bodies, box, T=T, **kw))
+            return made[-1]
+
+    r = _request(bench)
+    res = bench.trajectory_audit(NS, oracle, r)
+    assert res["flip_events"] >= bench.AUDIT_STEPS, res
+    o = oracle.OracleSimulation(r.bodies, r.box, T=np.float64, **r.kw).refresh()
+    nb = o.neighbors
+    ring1 = set(int(j) - 1 for j in nb.idx[:nb.count[100], 100])
+    ring2 = set(ring1)
+    for i in ring1:
+        ring2 |= set(int(j) - 1 for j in nb.idx[:nb.count[i], i])
+    assert 100 in ring2 and len(ring1) >= 5
+    assert res["bodies_charged"] >= len(ring2) - 2 and res["bodies_charged"] <= len(ring2) + 12, (res, len(ring2))
+    assert res["pass"], res
