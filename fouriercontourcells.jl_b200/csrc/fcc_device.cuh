@@ -90,6 +90,10 @@ struct GridSync {
     int error;        // 1: a barrier wait ran out (the kernel returned early)
     int any_need;     // some simulation rebuilds its neighbour list this step
     unsigned count2;  // arrivals at odd-numbered barriers
+    unsigned fexit;   // blocks done with a launch's flat step barriers
+    // flat step barriers of a lone simulation, by parity: arrivals (low 32
+    // bits) and skin votes (high 32 bits); zero between launches
+    unsigned long long fcnt[2];
 };
 
 template <class T>
@@ -325,6 +329,14 @@ __device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
 __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void red_add_release(unsigned long long* p, unsigned long long v) {
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
 
 #ifndef FCC_BARRIER_FENCE
 #define FCC_BARRIER_FENCE 0  // 1: full fence before the release store (measured: not needed, 1% slower)
@@ -345,6 +357,10 @@ struct BarrierLocal {
     int released;     // this block arrived last and released the barrier itself
     int err;          // this block's wait gave up
     unsigned bits;    // arrival bits summed up to this block's arrival
+    // flat step barriers (one simulation): arrivals and votes this block has
+    // seen complete on each parity's counter, and the next barrier's parity
+    unsigned ftgt[2], fvote[2];
+    int fpar;
 };
 
 // Generation word: bit 0 the released any_need flag, bits 1-8 the flags of a
@@ -363,6 +379,9 @@ __device__ __forceinline__ void barrier_start(GridSync* gs, BarrierLocal& bl, bo
         bl.rebuild = 0;
         bl.released = 0;
         bl.err = 0;
+        bl.ftgt[0] = bl.ftgt[1] = 0u;
+        bl.fvote[0] = bl.fvote[1] = 0u;
+        bl.fpar = 0;
     }
     __syncthreads();
 }
@@ -445,6 +464,59 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, BarrierLocal& bl, F&&
                                              A&& after = A{}, int tick = 0) {
     barrier_arrive(gs, bl, static_cast<F&&>(last), bits, static_cast<A&&>(after), tick);
     return barrier_wait<LIMIT>(gs, bl);
+}
+
+// Step barrier of a lone simulation without a releasing block: each block
+// adds its arrival and its skin vote (`vote`, into the high half) to the
+// counter of the barrier's parity with a release reduction, then polls the
+// counter until every block has arrived.  Every block thus reads the same
+// final value and runs the same bookkeeping on it, and the release costs one
+// trip to L2 instead of an atomic round trip, a store and a poll.  The value
+// read on completion is exact: a counter is next added to two step barriers
+// later, which no block reaches before every block has passed this one.  On
+// return (thread 0) bl.bits holds the votes of this barrier.  Counters run
+// from zero within a launch; flat_end clears them when the last block is
+// done.
+template <long long LIMIT = SPIN_LIMIT>
+__device__ __forceinline__ bool flat_barrier(GridSync* gs, BarrierLocal& bl, unsigned vote) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int p = bl.fpar;
+        unsigned long long* c = &gs->fcnt[p];
+        red_add_release(c, 1ull | ((unsigned long long)vote << 32));
+        const unsigned tgt = bl.ftgt[p] + gridDim.x;
+        bl.err = 0;
+        long long it = 0;
+        unsigned long long v;
+        while ((int)((unsigned)(v = ld_acquire(c)) - tgt) < 0) {
+            if (++it > LIMIT) {
+                atomicExch(&gs->error, 1);
+                bl.err = 1;
+                break;
+            }
+#if FCC_BARRIER_SLEEP > 0
+            __nanosleep(FCC_BARRIER_SLEEP);
+#endif
+        }
+        const unsigned hv = (unsigned)(v >> 32);
+        bl.bits = hv - bl.fvote[p];
+        bl.fvote[p] = hv;
+        bl.ftgt[p] = tgt;
+        bl.fpar = p ^ 1;
+    }
+    __syncthreads();
+    return bl.err == 0;
+}
+
+// End of a launch that used flat barriers (thread 0 of each block, after its
+// last wait): the last block to get here clears the counters for the next
+// launch; every block has then read them for the last time.
+__device__ __forceinline__ void flat_end(GridSync* gs) {
+    if (atomicAdd(&gs->fexit, 1u) == gridDim.x - 1) {
+        gs->fcnt[0] = 0ull;
+        gs->fcnt[1] = 0ull;
+        gs->fexit = 0u;
+    }
 }
 
 // Fast reciprocal square root for the FP32 force path (rsqrt, ~2 ulp);

@@ -661,6 +661,9 @@ constexpr int NBMAX = 12;
 #ifndef FCC_DYN
 #define FCC_DYN 1  // 1: FP32, one simulation: warps take their block's warp groups dynamically
 #endif
+#ifndef FCC_FLAT_BARRIER
+#define FCC_FLAT_BARRIER 1  // 1: a lone simulation's step barrier polls its arrival counter (flat_barrier)
+#endif
 
 // FP32 single-chunk kernels read cos(n phi_k), sin(n phi_k) (and n times
 // them) of their contour nodes from a shared-memory table instead of running
@@ -1991,6 +1994,23 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
         // a lone simulation that stepped ticks its block-local clock inside the
         // barrier: the next step's warps read it for their noise
         const int tick = (lone && (f0 & F_ACTIVE) && !(f0 & (F_FROZEN | F_HOLD))) ? 1 : 0;
+        if (FCC_FLAT_BARRIER && lone) {
+            // every block decides the next step from the same counter value;
+            // block 0 writes the global flags and clock
+            if (!flat_barrier(d.sync, bl, rb)) return;
+            if (threadIdx.x == 0) {
+                const int code = bookkeeping(d, bl, bl.bits, sim0);
+                if (blockIdx.x == 0) {
+                    d.sync->any_need = code & 1;
+                    lone_book_writes(d, bl, code);
+                }
+                bl.any = code & 1;
+                bl.flags = (code >> 1) & 0xff;
+                bl.clock += tick;
+            }
+            __syncthreads();
+            continue;
+        }
         if (!grid_barrier(
                 d.sync, bl, [&](unsigned rbs) { return bookkeeping(d, bl, rbs, sim0); }, rb,
                 [&](int code) {
@@ -1999,6 +2019,7 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
                 tick))
             return;
     }
+    if (FCC_FLAT_BARRIER && lone && threadIdx.x == 0) flat_end(d.sync);
 }
 
 // Self-test of the bounded barrier wait: the last block leaves without
