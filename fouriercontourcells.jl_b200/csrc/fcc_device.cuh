@@ -361,6 +361,7 @@ struct BarrierLocal {
     // seen complete on each parity's counter, and the next barrier's parity
     unsigned ftgt[2], fvote[2];
     int fpar;
+    int ovf;          // a neighbour list of this block overflowed in this rebuild
 };
 
 // Generation word: bit 0 the released any_need flag, bits 1-8 the flags of a

@@ -532,7 +532,7 @@ __device__ void phase_sort(const DevPtrs<T>& d, int tid, int nthr, const WorkLis
 constexpr int NB_LANES = 8, NB_PER = 8;
 template <class T>
 __device__ void phase_neighbors(const DevPtrs<T>& d, int par, int tid, int nthr, const SimDesc<T>* sim0,
-                                const WorkList* wl) {
+                                const WorkList* wl, int* overflow = nullptr) {
     constexpr unsigned FULL = 0xffffffffu;
     constexpr int BPW = 32 / NB_LANES, ROUND = NB_LANES * NB_PER;
     constexpr unsigned SUBMASK = (1u << NB_LANES) - 1u;
@@ -642,7 +642,10 @@ __device__ void phase_neighbors(const DevPtrs<T>& d, int par, int tid, int nthr,
         }
         if (act && h == 0) {
             d.nb_count[g] = n;
-            if (n > d.cap) atomicOr(&d.flags[s], F_FROZEN);
+            if (n > d.cap) {
+                atomicOr(&d.flags[s], F_FROZEN);
+                if (overflow) *overflow = 1;  // the block's vote at the closing flat barrier
+            }
             atomicMax(&d.maxcount[s], n);
             if (P->skin > T(0)) {
                 d.x0[g] = xi;
@@ -1863,6 +1866,30 @@ __device__ __forceinline__ bool rebuild_prologue(const DevPtrs<T>& d, int par, i
                                                  const SimDesc<T>* sim0, int* wl_area, int wl_cap) {
     // the phases set F_VALID / F_FROZEN: a lone simulation's flags are re-read
     auto keep = [&](unsigned) { return lone_sim(d) ? (bl.any | ((ldcg(d.flags) & 0xff) << 1)) : -1; };
+    if (FCC_FLAT_BARRIER && lone_sim(d)) {
+        // a lone simulation: flat barriers, and each block tracks the flags the
+        // phases set (F_VALID from the scan, F_FROZEN from an overflowing list,
+        // voted at the last barrier) instead of re-reading them
+        phase_count(d, par, tid, nthr, nullptr, bl.any);
+        if (!flat_barrier(d.sync, bl, 0u)) return false;
+        phase_scan(d, nullptr);
+        if (!flat_barrier(d.sync, bl, 0u)) return false;
+        phase_scatter(d, tid, nthr, nullptr);
+        if (!flat_barrier(d.sync, bl, 0u)) return false;
+        phase_sort(d, tid, nthr, nullptr);
+        if (!flat_barrier(d.sync, bl, 0u)) return false;
+        if (threadIdx.x == 0) bl.ovf = 0;
+        __syncthreads();
+        phase_neighbors(d, par, tid, nthr, sim0, nullptr, &bl.ovf);
+        __syncthreads();
+        if (!flat_barrier(d.sync, bl, bl.ovf ? 1u : 0u)) return false;
+        if (threadIdx.x == 0) {
+            bl.flags |= F_VALID;
+            if (bl.bits) bl.flags |= F_FROZEN;
+        }
+        __syncthreads();
+        return true;
+    }
     WorkList wl{};
     wl.m = -1;
     if (!sim0) wl = build_worklist(d, wl_area, wl_cap);
