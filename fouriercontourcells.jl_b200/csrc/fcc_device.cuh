@@ -477,10 +477,13 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, BarrierLocal& bl, F&&
 // later, which no block reaches before every block has passed this one.  On
 // return (thread 0) bl.bits holds the votes of this barrier.  Counters run
 // from zero within a launch; flat_end clears them when the last block is
-// done.
-template <long long LIMIT = SPIN_LIMIT>
-__device__ __forceinline__ bool flat_barrier(GridSync* gs, BarrierLocal& bl, unsigned vote) {
-    __syncthreads();
+// done.  `done` runs in thread 0 once the wait is over, before the closing
+// block barrier; `entry_sync` = false when the caller's own block barrier
+// just preceded the call (thread 0 alone may have worked since).
+template <long long LIMIT = SPIN_LIMIT, class F = NoAfter>
+__device__ __forceinline__ bool flat_barrier(GridSync* gs, BarrierLocal& bl, unsigned vote, F&& done = F{},
+                                             bool entry_sync = true) {
+    if (entry_sync) __syncthreads();
     if (threadIdx.x == 0) {
         const int p = bl.fpar;
         unsigned long long* c = &gs->fcnt[p];
@@ -504,6 +507,7 @@ __device__ __forceinline__ bool flat_barrier(GridSync* gs, BarrierLocal& bl, uns
         bl.fvote[p] = hv;
         bl.ftgt[p] = tgt;
         bl.fpar = p ^ 1;
+        if (!bl.err) done(0);
     }
     __syncthreads();
     return bl.err == 0;

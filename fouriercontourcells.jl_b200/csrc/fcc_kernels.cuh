@@ -2011,8 +2011,8 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
             if (!grid_barrier(d.sync, bl, [](unsigned) { return -1; })) return;
             for (int wg = g0 + warp; wg < g1; wg += WPB) update_warp_split<T, L>(d, wg, par, sim0, &bl.rebuild);
         }
-        __syncthreads();  // every warp's skin verdict is in bl.rebuild
-        const int f0 = bl.flags;
+        const int f0 = bl.flags;  // fixed during the step (read before thread 0 may rewrite it)
+        __syncthreads();          // every warp's skin verdict is in bl.rebuild
         unsigned rb = 0;
         if (threadIdx.x == 0) {  // reported with the arrival; cleared before the next forces phase
             rb = bl.rebuild ? 1u : 0u;
@@ -2024,8 +2024,8 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
         if (FCC_FLAT_BARRIER && lone) {
             // every block decides the next step from the same counter value;
             // block 0 writes the global flags and clock
-            if (!flat_barrier(d.sync, bl, rb)) return;
-            if (threadIdx.x == 0) {
+            // (the block barrier above is the flat barrier's entry barrier)
+            auto decide = [&](int) {
                 const int code = bookkeeping(d, bl, bl.bits, sim0);
                 if (blockIdx.x == 0) {
                     d.sync->any_need = code & 1;
@@ -2034,8 +2034,8 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
                 bl.any = code & 1;
                 bl.flags = (code >> 1) & 0xff;
                 bl.clock += tick;
-            }
-            __syncthreads();
+            };
+            if (!flat_barrier(d.sync, bl, rb, decide, false)) return;
             continue;
         }
         if (!grid_barrier(
