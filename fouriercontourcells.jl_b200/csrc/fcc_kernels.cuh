@@ -2049,15 +2049,18 @@ __global__ void __launch_bounds__(BLK, MINB) k_step(DevPtrs<T> d, int nsteps, in
     if (FCC_FLAT_BARRIER && lone && threadIdx.x == 0) flat_end(d.sync);
 }
 
-// Self-test of the bounded barrier wait: the last block leaves without
-// arriving, so the others wait for a release that never comes; after
-// SELFTEST_POLLS polls each records gs->error and returns.  Nothing else runs.
+// Self-test of the bounded barrier waits: the last block leaves without
+// arriving, so the others wait for a release that never comes, first at a
+// generation-word barrier on gs[0], then at a flat barrier on gs[1]; after
+// SELFTEST_POLLS polls each wait records its GridSync's error and returns.
+// Nothing else runs.
 constexpr long long SELFTEST_POLLS = 1ll << 14;
 __global__ void k_barrier_selftest(GridSync* gs) {
     __shared__ BarrierLocal bl;
     barrier_start(gs, bl, false, nullptr, nullptr);
     if (blockIdx.x == gridDim.x - 1) return;
     grid_barrier<SELFTEST_POLLS>(gs, bl, [](unsigned) { return -1; });
+    flat_barrier<SELFTEST_POLLS>(gs + 1, bl, 0u);
 }
 
 // compute_gradients! (src/simulation.jl:150-158): forces and every gradient

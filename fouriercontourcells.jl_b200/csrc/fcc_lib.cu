@@ -1591,10 +1591,10 @@ fcc_status fcc_health(fcc_sim* sim, int32_t* nonfinite, int32_t* barrier_error) 
 fcc_status fcc_barrier_selftest(int32_t blocks, int32_t* error, double* ms) {
     if (blocks < 1 || blocks > 148) return fail(FCC_ERR_ARGUMENT, "blocks must be 1..148");
     if (!error) return fail(FCC_ERR_ARGUMENT, "null argument");
-    GridSync* gs = nullptr;
-    CUDA_TRY(cudaMalloc(&gs, sizeof(GridSync)));
+    GridSync* gs = nullptr;  // [0]: generation-word barrier, [1]: flat barrier
+    CUDA_TRY(cudaMalloc(&gs, 2 * sizeof(GridSync)));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    cudaError_t e = cudaMemset(gs, 0, sizeof(GridSync));
+    cudaError_t e = cudaMemset(gs, 0, 2 * sizeof(GridSync));
     if (e == cudaSuccess) e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
     if (e == cudaSuccess) e = cudaEventRecord(e0, 0);
@@ -1604,15 +1604,16 @@ fcc_status fcc_barrier_selftest(int32_t blocks, int32_t* error, double* ms) {
     }
     if (e == cudaSuccess) e = cudaEventRecord(e1, 0);
     if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-    GridSync g{};
-    if (e == cudaSuccess) e = cudaMemcpy(&g, gs, sizeof(GridSync), cudaMemcpyDeviceToHost);
+    GridSync g[2]{};
+    if (e == cudaSuccess) e = cudaMemcpy(g, gs, 2 * sizeof(GridSync), cudaMemcpyDeviceToHost);
     float t = 0.f;
     if (e == cudaSuccess && ms) e = cudaEventElapsedTime(&t, e0, e1);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     cudaFree(gs);
     CUDA_TRY(e);
-    *error = g.error ? 1 : 0;
+    // 1: both waits ran out; 0: neither did; 2: only one of them did
+    *error = g[0].error && g[1].error ? 1 : (g[0].error || g[1].error ? 2 : 0);
     if (ms) *ms = t;
     return FCC_OK;
 }

@@ -28,13 +28,15 @@ def philox_noise(seed: int, draw: int, n: int, T=np.float64, lib=None, prefix="f
 
 
 def barrier_selftest(blocks: int = 4, lib=None):
-    """Run the self-test of the bounded grid-barrier wait: ``blocks`` blocks
-    of which one never arrives.  Returns (error, ms): error is True when the
-    others' wait ended with the error status (expected for blocks >= 2)."""
+    """Run the self-test of the bounded grid-barrier waits: ``blocks`` blocks
+    of which one never arrives, waited for at a generation-word barrier and
+    then at a flat barrier.  Returns (error, ms): error is 1 when both waits
+    ended with the error status (expected for blocks >= 2), 0 when neither
+    did, 2 when only one did."""
     lib = lib or native_library()
     err, ms = C.c_int32(), C.c_double()
     abi.check(lib.fcc_barrier_selftest(int(blocks), C.byref(err), C.byref(ms)), lib._lasterr)
-    return bool(err.value), ms.value
+    return int(err.value), ms.value
 
 
 def grid_dims(Lx, Ly, cutoff):

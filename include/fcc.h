@@ -281,12 +281,14 @@ fcc_status fcc_last_timing(fcc_sim* sim, double* ms, int64_t* launches, int64_t*
  * FCC_ERR_DEVICE). */
 fcc_status fcc_health(fcc_sim* sim, int32_t* nonfinite, int32_t* barrier_error);
 
-/* Self-test of the bounded grid-barrier wait (no counterpart in the
+/* Self-test of the bounded grid-barrier waits (no counterpart in the
  * reference): launches `blocks` blocks of which the last never arrives, so
- * the others' wait runs out after a fixed number of polls; *error = 1 when the
- * wait ended with the error status (the expected result for blocks >= 2; 0 for
- * one block, which waits for no one), *ms the kernel's duration.  The device
- * stays usable afterwards. */
+ * the others' waits run out after a fixed number of polls, first at a
+ * generation-word barrier (pools, parent drag), then at a flat barrier (the
+ * step barrier of a lone simulation); *error = 1 when both waits ended with
+ * the error status (the expected result for blocks >= 2), 0 when neither did
+ * (one block, which waits for no one), 2 when only one did; *ms the kernel's
+ * duration.  The device stays usable afterwards. */
 fcc_status fcc_barrier_selftest(int32_t blocks, int32_t* error, double* ms);
 
 /* ------------------------------------------------------------------ pool --

@@ -42,9 +42,9 @@ def test_nonfinite_state_is_flagged_and_cleared_by_set_state(T):
 
 def test_barrier_wait_runs_out_with_an_error_status():
     err, ms = fcc.barrier_selftest(1)  # one block waits for no one
-    assert not err
-    err, ms = fcc.barrier_selftest(4)  # the last block never arrives
-    assert err and 0 < ms < 10_000
+    assert err == 0
+    err, ms = fcc.barrier_selftest(4)  # the last block never arrives: both kinds of wait run out
+    assert err == 1 and 0 < ms < 10_000
     b, box, kw = small(5)  # the device is still usable
     s = fcc.Simulation(b, box, T=np.float32, **kw)
     s.run(20)
