@@ -827,6 +827,7 @@ struct Engine final : EngineBase {
     }
     // compiled user terms: the 8 x 5 / 256-thread kernels with the user-term code
     bool user = false;
+    bool owners_set = false;  // sim_of and cell_sim written (by the first load_state)
     void* step_kernel() const {
         if (user)
             return split ? (void*)k_step<T, 8, 5, true, true, 256, (sizeof(T) == 4 ? 2 : 1), true>
@@ -945,9 +946,12 @@ struct Engine final : EngineBase {
                 if (b->imgx) CUDA_TRY(cudaMemcpyAsync(imgx.p, b->imgx, n * sizeof(int), cudaMemcpyHostToDevice, stream));
                 if (b->imgy) CUDA_TRY(cudaMemcpyAsync(imgy.p, b->imgy, n * sizeof(int), cudaMemcpyHostToDevice, stream));
             }
-            CUDA_TRY(cudaMemsetAsync(sim_of.p, 0, n * sizeof(int), stream));
         }
-        CUDA_TRY(cudaMemsetAsync(cell_sim.p, 0, (size_t)ncx * ncy * sizeof(int), stream));
+        if (!owners_set) {  // every body and cell belongs to simulation 0; set once, at create
+            if (n) CUDA_TRY(cudaMemsetAsync(sim_of.p, 0, n * sizeof(int), stream));
+            CUDA_TRY(cudaMemsetAsync(cell_sim.p, 0, (size_t)ncx * ncy * sizeof(int), stream));
+            owners_set = true;
+        }
         const DevPtrs<T> d = ptrs();
         if (N > 0) {
             const int grid = (int)((N + INIT_BLOCK - 1) / INIT_BLOCK);
