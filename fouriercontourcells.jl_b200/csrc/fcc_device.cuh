@@ -515,7 +515,10 @@ __device__ __forceinline__ bool flat_barrier(GridSync* gs, BarrierLocal& bl, uns
 
 // End of a launch that used flat barriers (thread 0 of each block, after its
 // last wait): the last block to get here clears the counters for the next
-// launch; every block has then read them for the last time.
+// launch; every block has then read them for the last time.  A launch whose
+// wait ran out returns early and leaves them set; its error status stays set
+// too (every later step call fails) until fcc_set_state writes the whole
+// GridSync anew.
 __device__ __forceinline__ void flat_end(GridSync* gs) {
     if (atomicAdd(&gs->fexit, 1u) == gridDim.x - 1) {
         gs->fcnt[0] = 0ull;
