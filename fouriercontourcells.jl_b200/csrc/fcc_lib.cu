@@ -849,12 +849,13 @@ struct Engine final : EngineBase {
     // FP32, 7 in FP64) run a round in about 0.97 (FP32) or 0.945 (FP64) of the
     // time of 256-thread blocks but hold 12.5% fewer warps.  FP32 takes its
     // groups dynamically, so a step costs whole rounds: 224 wins where the
-    // 256-thread grid leaves its last round part-empty (N = 1024: 10.5 vs
-    // 11.1 µs, N = 16384: 25.1 vs 25.6 µs) and loses where both fill it
-    // (N = 65536: 91.3 vs 83.1 µs).  FP64 splits them statically, so a step
-    // costs the mean rounds per warp (at least one): 224 wins only while one
-    // round holds all groups (N = 1024: 14.8 vs 15.7 µs; N = 16384: 54.3 vs
-    // 52.0 µs).
+    // 256-thread grid leaves its last round part-empty (N = 1024: 9.57 vs
+    // 10.03 µs; N = 16384: 23.44 vs 23.45 µs, 61.4 vs 65.4 µs with a rebuild
+    // every step) and loses where both fill it (N = 65536: 88.1 vs 78.6 µs).
+    // FP64 splits them statically, so a step costs the mean rounds per warp
+    // (at least one): 224 wins only while one round holds all groups (N =
+    // 1024: 16.4 vs 16.6 µs; N = 16384: 63.1 vs 60.3 µs).  (Deformed states
+    // after 300 warm-up steps, flat step barrier.)
     fcc_status choose_variant() {
         variant = 0;
         if (user) {  // one kernel family carries the user-term code
