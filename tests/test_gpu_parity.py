@@ -431,6 +431,25 @@ def test_run_equals_step_bitwise():
     assert same(e, f)
 
 
+def test_fp32_monolayer_overflow_regrows_inside_runs():
+    """The FP32 step kernel of a lone monolayer (no parent drag: the fused
+    step and its own rebuild phases) with a neighbour capacity of 1: lists
+    overflow inside multi-step launches, the launch stops stepping, the host
+    regrows and reruns the missing steps; the result equals step-by-step
+    launches and a run with room from the start, bit for bit
+    (src/neighbors.jl:226-233, test/test_cuda.jl:133-185)."""
+    bodies, box = fcc.hexagonal_monolayer(12, 12, packing=0.97, maxmode=10, rng=3)
+    bodies.coef[1:, :] = 0.03 * np.random.default_rng(8).standard_normal((bodies.ncoef - 1, bodies.n))
+    kw = dict(types=(fcc.BodyType(v0=1.0, Dr=0.5, μab=0.1),), energies=(fcc.Tension(0.01), fcc.Overlap(1.0)),
+              dt=0.005, seed=11, skin=0.05, T=np.float32)
+    a = G(bodies, box, nl_capacity=1, **kw).run(120)
+    b = G(bodies, box, nl_capacity=1, **kw).step(120)
+    c = G(bodies, box, **kw).run(120)
+    assert a.neighbors.cap > 1 and a.builds > 5
+    assert same(a, b)
+    assert all(np.array_equal(u, v) for u, v in zip(state(a), state(c)))
+
+
 def test_skin_zero_rebuilds_every_step_and_agrees():
     """test/test_contact.jl:155-160: skin 0 vs 0.5 agree to 1e-10."""
     bodies, box = fcc.hexagonal_monolayer(6, 6, packing=0.97, rng=2)
