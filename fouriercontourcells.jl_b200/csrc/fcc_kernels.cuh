@@ -6,8 +6,10 @@
 //   forces + Euler-Maruyama update fused per body (no parent drag), or
 //   forces | barrier | displacement + update (parent drag: a body's motion
 //   needs its children's forces)
-//   grid barrier whose last block ticks the clocks and decides the next
-//   rebuild (the device-side form of update_neighbors!'s skin check).
+//   grid barrier that ticks the clocks and decides the next rebuild (the
+//   device-side form of update_neighbors!'s skin check): for a lone
+//   simulation every block decides from the same arrival counter (flat
+//   barrier), for a pool the last block to arrive decides and releases.
 //
 // Work mapping of the force evaluation: L lanes per body (L = 8 for nθ = 40),
 // 32/L bodies per warp; lane l owns contour nodes k = l + L*s, s < S, so a
@@ -1803,22 +1805,23 @@ __device__ __forceinline__ int book_one(const DevPtrs<T>& d, int s) {
 }
 
 // A launch that advances one simulation with no step limit: its flags and
-// clock are known to every block (released with each barrier, ticked
-// locally), so the bookkeeping needs no global reads.
+// clock are known to every block (decided by every block at each flat
+// barrier, ticked locally), so the bookkeeping needs no global reads.
 template <class T>
 __device__ __forceinline__ bool lone_sim(const DevPtrs<T>& d) {
     return d.nsims == 1 && d.stop == nullptr;
 }
 
-// Last block of a step's closing barrier: tick the clocks of the simulations
-// that stepped and decide the rebuilds of the next step (skin exceeded, list
+// End of a step's closing barrier: tick the clocks of the simulations that
+// stepped and decide the rebuilds of the next step (skin exceeded, list
 // invalid, or skin = 0: src/simulation.jl:132-142).  Returns (in thread 0)
-// the release code: whether some simulation rebuilds at the next step, and
-// for a lone simulation its new flags (<< 1).  `rebuilds`: blocks whose
-// bodies exceeded their skin in this step.
-// A lone simulation's decision needs no global memory (its flags are in the
-// barrier word, its descriptor `P` in shared memory); its global flags and
-// clock are written after the release (lone_book_writes).
+// the code: whether some simulation rebuilds at the next step, and for a
+// lone simulation its new flags (<< 1).  `rebuilds`: blocks whose bodies
+// exceeded their skin in this step.  A pool's last block to arrive runs it
+// before releasing the barrier; for a lone simulation every block runs it on
+// the flat barrier's counter value, with no global memory (its flags are
+// block-local, its descriptor `P` in shared memory), and block 0 writes its
+// global flags and clock (lone_book_writes).
 template <class T>
 __device__ int bookkeeping(const DevPtrs<T>& d, const BarrierLocal& bl, unsigned rebuilds, const SimDesc<T>* P) {
     if (lone_sim(d)) {
@@ -1843,11 +1846,12 @@ __device__ int bookkeeping(const DevPtrs<T>& d, const BarrierLocal& bl, unsigned
     return s_any;
 }
 
-// The global side of a lone simulation's bookkeeping, after the release: the
-// host reads the clock and flags after the launch, the rebuild phases read
-// F_NEED only after the first rebuild barrier (phase_count takes the decision
-// from the barrier word).  The flag updates are atomic: they keep the bits
-// other blocks set (non-finite, overflow).
+// The global side of a lone simulation's bookkeeping, written by one block
+// once the step barrier is passed: the host reads the clock and flags after
+// the launch, the rebuild phases read F_NEED only after the first rebuild
+// barrier (phase_count takes the decision from the block's own copy).  The
+// flag updates are atomic: they keep the bits other blocks set (non-finite,
+// overflow).
 template <class T>
 __device__ __forceinline__ void lone_book_writes(const DevPtrs<T>& d, const BarrierLocal& bl, int code) {
     const int f = bl.flags;
