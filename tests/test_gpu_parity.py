@@ -6,8 +6,9 @@ Inputs are identical for both sides; tolerances are stated per test:
 - cell and neighbour lists: bit-exact at equal precision on equal inputs;
 - forces/gradients and one-step updates: max error / max magnitude per field
   <= 1e-12 in FP64, <= 1e-5 in FP32 (FP32 compared against the FP64 oracle on
-  FP32-representable inputs, bodies at an Overlap near-tie |d| < 1e-4
-  excluded and counted: the Heaviside g = J H(d) flips there);
+  FP32-representable inputs, bodies at an Overlap near-tie excluded and
+  counted: the Heaviside g = J H(d) flips there; a one-step θ also carries
+  the difference between the Float32 and Float64 rotational noise draws);
 - trajectories: the reference's golden N = 64 run at atol 1e-10
   (test/test_dynamics.jl:53-70), 30 noisy FP64 steps at rtol 1e-8 with equal
   rebuild counts (test/test_cuda.jl:123-131);
@@ -584,6 +585,43 @@ def test_n16384_fp32_forces_vs_oracle():
     assert keep.mean() > 0.95
     for f in ("gx", "gy", "gθ", "gcoef", "Ebody"):
         assert relerr(getattr(g.grad, f), getattr(o.grad, f), keep) < 1e-5, f
+
+
+def test_n16384_fp32_one_step_vs_fp64_oracle():
+    """One FP32 step of the N = 16384 workload through the fused step kernel
+    (deformed by 200 steps; its own list rebuild and Philox draw) against one
+    FP64 oracle step from the same FP32 state and clock: every increment
+    within 1e-5 of its field's increment scale plus 2 FP32 ulp of the state,
+    bodies at an Overlap near-tie excluded (at most 5%).  The rotational
+    noise is the reference's Float32 draw (24-bit uniforms) on one side and
+    its Float64 draw on the other: θ is also allowed the difference of the
+    two draws times the noise amplitude sqrt(2 Dr dt) (it reaches 2e-5 of
+    the increment where the Box-Muller radius uniform is small)."""
+    bodies, box = c2_bodies()
+    kw = dict(types=C2_TYPES, energies=C2_ENERGIES, dt=0.005, seed=1234)
+    g = G(bodies, box, T=np.float32, **kw)
+    g.run(200)
+    state, clk = g.bodies, g.clock
+    o = O(state, box, T=np.float64, **kw)
+    o.set_state(state, clock=clk)
+    o.refresh()
+    keep = ~near_ties(o)
+    assert keep.mean() > 0.95
+    g.set_state(state, clock=clk)
+    g.step(1)
+    o.step(1)
+    assert g.clock == o.clock == clk + 1
+    bg, bo = g.bodies, o.bodies
+    z32, z64 = fcc.philox_noise(1234, clk, bodies.n, np.float32), fcc.philox_noise(1234, clk, bodies.n, np.float64)
+    noise = {"θ": math.sqrt(2 * C2_TYPES[0].Dr * 0.005) * np.abs(z32[2] - z64[2])}
+    for f in ("x", "y", "θ", "coef"):
+        sg, so, s0 = getattr(bg, f), getattr(bo, f), getattr(state, f)
+        dg, do = sg - s0, so - s0
+        tol = 1e-5 * np.abs(do).max() + 2 * np.spacing(np.abs(so).astype(np.float32)).astype(np.float64)
+        tol = tol + noise.get(f, 0.0)
+        err = np.abs(dg - do)[..., keep]
+        assert (err <= tol[..., keep]).all(), (f, float((err / tol[..., keep]).max()))
+    assert np.array_equal(bg.imgx, bo.imgx) and np.array_equal(bg.imgy, bo.imgy)
 
 
 @pytest.mark.parametrize("nx", [128, 256, 512])
