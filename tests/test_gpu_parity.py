@@ -624,6 +624,41 @@ def test_n16384_fp32_one_step_vs_fp64_oracle():
     assert np.array_equal(bg.imgx, bo.imgx) and np.array_equal(bg.imgy, bo.imgy)
 
 
+def test_n16384_fp64_forces_and_one_step_match_oracle():
+    """The N = 16384 workload in FP64 (deformed by 200 steps on the GPU):
+    every gradient field of the state at 1e-12 of its scale, then one step
+    from the same state and clock with increments at 1e-12 of their scale
+    plus two ulp of the state (positions up to 250: one ulp of the sum
+    x + dx is 6e-14); neighbour counts identical."""
+    bodies, box = c2_bodies()
+    kw = dict(types=C2_TYPES, energies=C2_ENERGIES, dt=0.005, seed=1234, T=np.float64)
+    g = G(bodies, box, **kw)
+    g.run(200)
+    state, clk = g.bodies, g.clock
+    o = O(state, box, **kw)
+    o.set_state(state, clock=clk)
+    g.set_state(state, clock=clk)
+    g.refresh()
+    o.refresh()
+    assert np.array_equal(g.neighbors.count, o.neighbors.count)
+    keep = ~near_ties(o, 1e-12)  # FP64 rounding decides a Heaviside only this close to a tie
+    assert keep.mean() > 0.999
+    for f in ("gx", "gy", "gθ", "gcoef", "Ebody"):
+        assert relerr(getattr(g.grad, f), getattr(o.grad, f), keep) < 1e-12, f
+    g.set_state(state, clock=clk)
+    o.set_state(state, clock=clk)
+    g.step(1)
+    o.step(1)
+    bg, bo = g.bodies, o.bodies
+    for f in ("x", "y", "θ", "coef"):
+        sg, so, s0 = getattr(bg, f), getattr(bo, f), getattr(state, f)
+        dg, do = sg - s0, so - s0
+        tol = 1e-12 * np.abs(do).max() + 2 * np.spacing(np.abs(so))
+        err = np.abs(dg - do)[..., keep]
+        assert (err <= tol[..., keep]).all(), (f, float((err / tol[..., keep]).max()))
+    assert np.array_equal(bg.imgx, bo.imgx) and np.array_equal(bg.imgy, bo.imgy)
+
+
 @pytest.mark.parametrize("nx", [128, 256, 512])
 def test_full_size_invariants(nx):
     """N = 16384, 65536, 262144 FP32: finite state, area πR0² kept by the FP64
